@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 cell-updates/s of the SSP-RK2 shallow-water step.
+
+Workload (N = 1): 2048 x 2048 Cartesian cells, dx = 2 m, FP64: wet/dry dam
+break over a seeded sloping beach (1:50 plus 0.3 m smooth noise), dry land
+initially, Manning n = 0.03, Flather open boundary on the west side, walls
+elsewhere; each step takes dt = maxDt() (CFL 0.45).  One "step" is one full
+SSP-RK2 step of the whole grid: 2048 * 2048 cell-updates.  The device holds
+b, two copies of (h, hu, hv) and the metric, about 236 MB -- larger than the
+126 MB L2, so nothing is flushed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (torchrun, one process per GPU): every rank advances its own
+independent basin of the same size (weak scaling, no data-path collective);
+the timed region is bracketed by a barrier and the max over ranks is taken.
+
+--impl reference times the CPU restatement of the reference solver (the
+oracle; the reference itself is JavaScript and no JS engine exists on the
+box) with every host thread, on a bounded sample of the same workload.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = 2048
+DX = 2.0
+MANNING = 0.03
+METRIC = "FP64 cell-updates/s"
+UNIT = "cell-updates/s"
+STAGE_BYTES = {"stage1": 56, "stage2": 80}      # algorithmic HBM bytes per cell per launch
+STEP_BYTES = 136                                # per cell-update (both stages)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload():
+    import __graft_entry__
+    swe = __graft_entry__.load_package()
+    from water_simulator_b200.workloads import beach_dam_break
+    b, eta = beach_dam_break(NX, NY, DX)
+    return swe, b, eta
+
+
+def config(extra=None):
+    c = {"workload": "cartesian 2048x2048 dx=2 m wet/dry dam break over a seeded 1:50 beach, "
+                     "Manning 0.03, Flather west, dt = maxDt()",
+         "nx": NX, "ny": NY, "cells_per_step": NX * NY, "l2": "inputs larger than L2 (236 MB resident)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the stage-2 kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "k_stage2_beach2048.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.gpu = gpu_index
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(gpu_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_oracle_sim(b, eta, threads):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_sim import OracleSim
+    sim = OracleSim(nx=NX, ny=NY, dx=DX, bed=b, eta0=eta, manning=MANNING, threads=threads)
+    sim.set_boundaries(west=("flather", lambda t: 0.0, lambda t: 0.0), east="reflect",
+                       south="reflect", north="reflect")
+    return sim
+
+
+def cpu_baseline(b, eta, threads=1, budget_s=12.0, max_steps=30):
+    """The oracle on the host cores: steps of the same workload until the
+    time budget is used (at least one)."""
+    sim = cpu_oracle_sim(b, eta, threads)
+    sim.step()                      # warm (first touch)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        sim.step()
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or n >= max_steps:
+            break
+    return {"value": NX * NY * n / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} self-timed steps of the 2048x2048 workload ({el:.1f} s) on the oracle "
+                      f"(C++ restatement of src/swe.mjs), {threads} thread(s)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    _, b, eta = workload()
+    threads = os.cpu_count() or 1
+    sim = cpu_oracle_sim(b, eta, threads)
+    for _ in range(max(args.warmup, 0)):
+        sim.step()
+    steps = max(1, min(args.steps, 20))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step()
+    el = time.perf_counter() - t0
+    v = NX * NY * steps / el
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": config({"threads": threads}),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{steps} self-timed steps of the 2048x2048 workload on the oracle "
+                                       f"(C++ restatement of src/swe.mjs; the reference is JavaScript and "
+                                       f"no JS engine exists here), {threads} OpenMP threads"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def make_sim(swe, b, eta):
+    sim = swe.ShallowWater(nx=NX, ny=NY, dx=DX, bed=b, eta0=eta, manning=MANNING)
+    sim.boundaries = {"west": swe.flather(lambda t: 0.0, lambda t: 0.0), "east": swe.reflect,
+                      "south": swe.reflect, "north": swe.reflect}
+    return sim
+
+
+def run_ours(args):
+    rank, world, local = dist_env()
+    import torch
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    swe, b, eta = workload()
+    lib = swe.load_library()
+    swe._lib.check(lib.swe_set_device(local))
+    sim = make_sim(swe, b, eta)
+    stream_ptr = ctypes.c_void_p()
+    swe._lib.check(lib.swe_get_stream(sim._h, ctypes.byref(stream_ptr)))
+    stream = torch.cuda.ExternalStream(stream_ptr.value, device=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # warm-up: W steps through the device loop (also builds the CUDA graph)
+    sim.run(max(args.warmup, 3))
+    sim.synchronize()
+    K = args.steps
+    sim.run(min(K, 32))             # same graph shape as the timed loop
+    sim.synchronize()
+
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    done = sim.run(K)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    barrier()
+    if done != K:
+        raise RuntimeError(f"the device loop took {done} of {K} steps")
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * NX * NY * K / (ms_max / 1e3)
+
+    # per-launch durations (events between launches on the library's stream)
+    dt = sim.maxDt()
+    phases = {"prepare": [], "bc1": [], "stage1": [], "bc2": [], "stage2": []}
+    msv = (ctypes.c_double * 5)()
+    for _ in range(20):
+        swe._lib.check(lib.swe_step_timed(sim._h, dt, msv))
+        for key, v in zip(phases, msv):
+            phases[key].append(v)
+    avg = {k: statistics.mean(v[2:]) for k, v in phases.items()}
+    step_ms = sum(avg.values())
+    peak, peak_kind = measured_peaks()
+    st2_bytes = STAGE_BYTES["stage2"] * NX * NY
+    achieved = st2_bytes / (avg["stage2"] / 1e3) / 1e9
+    traffic = profile_traffic()
+    roofline = {"bound": "hbm", "kernel": "k_stage<2> (stage 2 + friction + sponge + CFL epilogue)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                "fallback 6.65 TB/s",
+                "traffic": traffic, "algorithmic_bytes_per_launch": st2_bytes,
+                "avg_launch_ms": avg["stage2"],
+                "step_phase_ms": avg,
+                "note": "FP64-issue bound: the kernel's ceiling is the FP64 pipe, not HBM; see DESIGN.md"}
+
+    # e2e through the C ABI with host buffers: per step upload (h, hu, hv)
+    # from pinned host memory, one self-timed step, download (h, hu, hv).
+    N = (NX + 4) * (NY + 4)
+    pinned = [torch.empty(N, dtype=torch.float64).pin_memory() for _ in range(3)]
+    for q, f in enumerate(("h", "hu", "hv")):
+        pinned[q].numpy()[:] = sim.field(f)
+    ptrs = [ctypes.cast(p.data_ptr(), ctypes.POINTER(ctypes.c_double)) for p in pinned]
+    e2e_steps = max(3, min(K, 40))
+    taken = ctypes.c_double()
+
+    def e2e_step():
+        for q in range(3):
+            swe._lib.check(lib.swe_set_field(sim._h, 1 + q, ptrs[q]))
+        swe._lib.check(lib.swe_step_auto(sim._h, ctypes.byref(taken)))
+        for q in range(3):
+            swe._lib.check(lib.swe_get_field(sim._h, 1 + q, ptrs[q]))
+
+    e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * NX * NY * e2e_steps / float(t.item())
+
+    # device-resident drop-in use: the driver loop sim.step(sim.maxDt())
+    # with the state on the device and dt crossing to the host each step
+    t0 = time.perf_counter()
+    res_steps = max(3, min(K, 200))
+    for _ in range(res_steps):
+        swe._lib.check(lib.swe_step_auto(sim._h, ctypes.byref(taken)))
+    sim.synchronize()
+    res_value = NX * NY * res_steps / (time.perf_counter() - t0)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(b, eta, threads=1)
+
+    if world > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+                "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "config": config({"parallelism": f"independent basin per GPU x{world}",
+                                  "launch": dict(zip(["grid_x", "grid_y", "threads", "cols_per_cta",
+                                                      "rows_per_cta"], launch_cfg(swe, lib, sim)))}),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * N * 8,
+                        "d2h_bytes_per_step": 3 * N * 8 + 8,
+                        "how": "per step: swe_set_field x3 from pinned host memory, swe_step_auto, "
+                               "swe_get_field x3 into pinned host memory"},
+                "e2e_resident": {"value": res_value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                 "d2h_bytes_per_step": 8,
+                                 "how": "per step: swe_step_auto (dt = maxDt read back), state on the device"},
+                "gpu_launches": 5 * K,
+                "roofline": roofline, "clocks": clocks, "cpu_baseline": cpu,
+                "hbm_bytes_per_cell_update": STEP_BYTES}
+        print(json.dumps(line))
+    sim.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def launch_cfg(swe, lib, sim):
+    cfg = (ctypes.c_int * 5)()
+    swe._lib.check(lib.swe_get_launch_config(sim._h, cfg))
+    return list(cfg)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

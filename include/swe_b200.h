@@ -1,0 +1,210 @@
+/*
+ * swe_b200.h -- C ABI of the B200 shallow-water step library (libswe_b200.so).
+ *
+ * Drop-in boundary for the hot path of Syntaxswine/water-simulator: the
+ * well-balanced finite-volume step of `ShallowWater` (src/swe.mjs) and its
+ * spherical metric (src/geometry.mjs).  Host code (a Node N-API addon, the
+ * Python mirror in water-simulator_b200/, or plain C) keeps the reference's
+ * object model and calls these entry points; the library owns the device
+ * buffers, the caller owns every host array and the library copies in and out.
+ *
+ * Conventions
+ *   - Arrays are FP64, row-major over the padded grid W = nx + 4 by H = ny + 4
+ *     (two ghost rings), index k = j*W + i, exactly as the reference's
+ *     Float64Array fields (src/swe.mjs:196-220, 268).
+ *   - Every function returns SWE_OK (0) or a negative status; the message of
+ *     the last failure on the calling thread is swe_last_error().  Nothing
+ *     aborts or traps.  Errors the reference throws (unknown limiter, bad
+ *     latitudes, odd nx at a pole, bad Manning n) come back as SWE_EINVAL
+ *     with the reference's message.
+ *   - Each handle owns one CUDA stream; calls on one handle are synchronous
+ *     with respect to the host data they return and must come from one
+ *     thread at a time (the reference is single-threaded, src/swe.mjs:968).
+ *   - There is no CPU fallback: if no CUDA device is usable, swe_create fails
+ *     with SWE_ECUDA.
+ */
+#ifndef SWE_B200_H
+#define SWE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWE_OK          0
+#define SWE_EINVAL     -1   /* bad argument; the reference would throw */
+#define SWE_ECUDA      -2   /* CUDA runtime failure or no device */
+#define SWE_ENONFINITE -3   /* a field went non-finite */
+#define SWE_ETIMEOUT   -4   /* a bounded device wait gave up */
+
+#define SWE_LIMITER_MC      0   /* src/swe.mjs:133 (default) */
+#define SWE_LIMITER_MINMOD  1   /* src/swe.mjs:88 */
+#define SWE_LIMITER_CENTRAL 2   /* src/swe.mjs:141 */
+
+#define SWE_SIDE_WEST  0        /* side numbering of src/swe.mjs:1023 */
+#define SWE_SIDE_EAST  1
+#define SWE_SIDE_SOUTH 2
+#define SWE_SIDE_NORTH 3
+
+#define SWE_BC_REFLECT  0       /* reflect,  src/swe.mjs:1026 */
+#define SWE_BC_OUTFLOW  1       /* outflow,  src/swe.mjs:1042 */
+#define SWE_BC_PERIODIC 2       /* periodic, src/swe.mjs:1119 */
+#define SWE_BC_FLATHER  3       /* flather,  src/swe.mjs:1085 */
+
+/* field ids for swe_get_field / swe_set_field (src/swe.mjs:200-220) */
+#define SWE_FIELD_B       0
+#define SWE_FIELD_H       1
+#define SWE_FIELD_HU      2
+#define SWE_FIELD_HV      3
+#define SWE_FIELD_H0      4     /* readable after a step with keep_h0 on */
+#define SWE_FIELD_HU0     5
+#define SWE_FIELD_HV0     6
+#define SWE_FIELD_RH      7     /* readable after swe_residual */
+#define SWE_FIELD_RHU     8
+#define SWE_FIELD_RHV     9
+#define SWE_FIELD_THETA  10
+#define SWE_FIELD_MANNING 11
+
+/* metric row ids for swe_get_geom / swe_set_geom (src/geometry.mjs:301-309) */
+#define SWE_GEOM_DXROW    0
+#define SWE_GEOM_DYROWN   1
+#define SWE_GEOM_DYROWS   2
+#define SWE_GEOM_DYCFL    3
+#define SWE_GEOM_AREA     4
+#define SWE_GEOM_LX       5
+#define SWE_GEOM_LYN      6
+#define SWE_GEOM_LYS      7
+#define SWE_GEOM_BEDPHI   8
+#define SWE_GEOM_PHIC     9
+#define SWE_GEOM_TANPHI  10
+#define SWE_GEOM_FROW    11
+#define SWE_GEOM_GEOCOEF 12
+#define SWE_GEOM_NROWS   13
+
+/* scalar ids for swe_get_scalar / swe_set_scalar */
+#define SWE_SCALAR_DX          0   /* NaN on a sphere (src/swe.mjs:185) */
+#define SWE_SCALAR_DY          1
+#define SWE_SCALAR_R           2   /* Infinity in Cartesian */
+#define SWE_SCALAR_DLAM        3
+#define SWE_SCALAR_DPHI        4
+#define SWE_SCALAR_TOTAL_AREA  5
+#define SWE_SCALAR_T           6   /* settable */
+#define SWE_SCALAR_STEPS       7   /* settable */
+#define SWE_SCALAR_MASS_FLOORED 8
+#define SWE_SCALAR_EPS4        9
+
+/* Constructor options, src/swe.mjs:170-174 (+ the `sphere` object,
+ * src/geometry.mjs:190-192).  swe_options_init fills the reference defaults. */
+typedef struct swe_options {
+  int    nx, ny;
+  double dx, dy;
+  double manning;      /* 0.025 */
+  double min_depth;    /* 1e-3 */
+  double cfl;          /* 0.45 */
+  double coriolis;     /* 0 */
+  int    order;        /* 2 */
+  int    limiter;      /* SWE_LIMITER_MC */
+  int    sphere;       /* 0 Cartesian, 1 latitude-longitude */
+  double R, lat0, lat1, omega;   /* sphere: 6371e3, -90, 90, 0 */
+} swe_options;
+
+typedef struct swe_sim swe_sim;
+
+/* Select the CUDA device for handles created afterwards on this thread
+ * (one process per GPU: rank r calls swe_set_device(r)). */
+int swe_set_device(int ordinal);
+
+/* Defaults of src/swe.mjs:170-174. */
+int swe_options_init(swe_options* o);
+
+/* new ShallowWater(opts), src/swe.mjs:170-244.  b and h are the sampled
+ * bed and depth over the padded grid (the caller samples bed()/eta0() per
+ * cell including ghosts, src/swe.mjs:222-232); hu = hv = 0.  Boundaries
+ * default as the reference's (src/swe.mjs:239-241). */
+int swe_create(const swe_options* o, const double* b, const double* h, swe_sim** out);
+int swe_destroy(swe_sim* s);
+const char* swe_last_error(void);
+/* W, H, nx, ny */
+int swe_get_dims(swe_sim* s, int* dims4);
+
+/* sim.b / sim.h / ... reads and writes (src/swe.mjs:200-220). */
+int swe_get_field(swe_sim* s, int field, double* out);
+int swe_set_field(swe_sim* s, int field, const double* in);
+/* sim.geom.* rows (src/geometry.mjs:301-309); writes take effect from the
+ * next device call, as a JS write to geom rows does (tools/verify-sphere.mjs:569). */
+int swe_get_geom(swe_sim* s, int row, double* out);
+int swe_set_geom(swe_sim* s, int row, const double* in);
+int swe_get_scalar(swe_sim* s, int which, double* out);
+int swe_set_scalar(swe_sim* s, int which, double v);
+
+/* sim.boundaries.<side> = reflect | outflow | periodic | flather(...),
+ * src/swe.mjs:1026-1126. */
+int swe_set_boundary(swe_sim* s, int side, int kind);
+/* flather(etaExt, uExt): the two values etaExt(sim.t), uExt(sim.t) for the
+ * next step (they depend on t only, src/swe.mjs:1093). */
+int swe_set_flather_values(swe_sim* s, int side, double eta_ext, double u_ext);
+/* flather driven by a harmonic table evaluated on the device each step:
+ * eta(t) = msl + sum amp[q] cos(omega[q] t - phase_deg[q] pi/180)
+ * (Tide.eta, src/tide.mjs:103-107), u(t) = u_coef * eta(t). n <= 16. */
+int swe_set_flather_tide(swe_sim* s, int side, double msl, int n, const double* amp,
+                         const double* omega, const double* phase_deg, double u_coef);
+/* setManningField, src/swe.mjs:714-731 (array form; NULL clears). */
+int swe_set_manning_field(swe_sim* s, const double* n);
+/* sim.forcing = makeSponge(sim, {side, width, strength, etaRef}),
+ * src/swe.mjs:1174-1198, run on the device after friction. */
+int swe_set_sponge(swe_sim* s, int side, int width, double strength, double eta_ref);
+int swe_clear_sponge(swe_sim* s);
+/* Keep a copy of the step's starting state readable as SWE_FIELD_H0.. */
+int swe_set_keep_h0(swe_sim* s, int on);
+
+/* applyBC(), src/swe.mjs:289-303 */
+int swe_apply_bc(swe_sim* s);
+/* residual(dt), src/swe.mjs:308-629: fills RH, RHU, RHV, THETA. */
+int swe_residual(swe_sim* s, double dt);
+/* maxDt(), src/swe.mjs:632-647 (Infinity when no cell is wet). */
+int swe_max_dt(swe_sim* s, double* out);
+/* applyFriction(dt), src/swe.mjs:659-704 */
+int swe_apply_friction(swe_sim* s, double dt);
+/* dryClean(), src/swe.mjs:734-745 */
+int swe_dry_clean(swe_sim* s, double* added);
+/* step(dt), src/swe.mjs:754-814: *taken = dt, or 0 when dt is not > 0 or not finite. */
+int swe_step(swe_sim* s, double dt, double* taken);
+/* step() with no argument: dt = maxDt(). */
+int swe_step_auto(swe_sim* s, double* taken);
+/* The drivers' loop `while (...) sim.step(...)` kept on the device: n steps
+ * of dt = dt_fixed (if > 0) or maxDt(), each clamped to t_end - t
+ * (t_end = +Infinity for none); stops early, like the loop, at the first
+ * refused step.  *done = steps taken.  Launched as CUDA graphs. */
+int swe_run(swe_sim* s, int n, double dt_fixed, double t_end, int* done);
+
+/* Diagnostics, src/swe.mjs:819-917 (same summation order as the reference). */
+int swe_volume(swe_sim* s, double* out);
+int swe_energy(swe_sim* s, double* out);
+int swe_max_surface_deviation(swe_sim* s, double ref, double* out);
+int swe_max_speed(swe_sim* s, double* out);
+int swe_finite(swe_sim* s, int* out);
+int swe_synchronize(swe_sim* s);
+/* The handle's CUDA stream (a cudaStream_t), so a caller can record CUDA
+ * events on the stream the kernels run on. */
+int swe_get_stream(swe_sim* s, void** stream);
+/* step(dt) with CUDA events between its five launches (prepare, ghost fill,
+ * stage 1, ghost fill, stage 2); ms[5] receives each launch's duration. */
+int swe_step_timed(swe_sim* s, double dt, double* ms);
+/* Launch shape of the stage kernel: grid x, grid y, threads, output
+ * columns per CTA, output rows per CTA. */
+int swe_get_launch_config(swe_sim* s, int* cfg5);
+
+/* cartesianGeometry / sphericalGeometry (src/geometry.mjs:163-299) as a
+ * host-side set-up call, no device needed: fills rows[13*H] (row id major)
+ * and scalars[6] (SWE_SCALAR_DX .. SWE_SCALAR_TOTAL_AREA). */
+int swe_compute_geometry(const swe_options* o, double* rows, double* scalars);
+
+/* The exported hllc (src/swe.mjs:975) over a batch, on the device:
+ * in = n x (hL, huL, hvL, hR, huR, hvR, dry), out = n x 3. */
+int swe_hllc_batch(int n, const double* in, double* out);
+/* sim.vel(hq, h) (src/swe.mjs:282) over a batch, on the device. */
+int swe_vel_batch(swe_sim* s, int n, const double* hq, const double* h, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

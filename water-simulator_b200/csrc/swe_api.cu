@@ -1,0 +1,900 @@
+// swe_api.cu -- host side of libswe_b200.so: the C ABI declared in
+// include/swe_b200.h.  Owns device buffers and one CUDA stream per
+// simulation, sets up the metric (src/geometry.mjs), and sequences the
+// kernels of swe_kernels.cuh.  No CPU solver path exists here: every field
+// update runs on the GPU.
+#include "../../include/swe_b200.h"
+#include "swe_kernels.cuh"
+
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <cstddef>
+#include <cstdlib>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) { g_err = msg; return code; }
+
+#define CU(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(SWE_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+const double PI = 3.141592653589793;
+const double HALF_PI = PI / 2;
+
+// ---- metric, src/geometry.mjs ------------------------------------------------
+double js_max(double a, double b) { return swe::jmax(a, b); }
+double js_min(double a, double b) { return swe::jmin(a, b); }
+double clamp_lat(double p) { return p > HALF_PI ? HALF_PI : p < -HALF_PI ? -HALF_PI : p; }      // :111
+double reflect_lat(double p) { return p > HALF_PI ? PI - p : p < -HALF_PI ? -PI - p : p; }    // :112
+double cos_lat(double p) {                                                                     // :153
+  const double co = HALF_PI - std::fabs(p);
+  return co <= 0 ? 0 : std::sin(co);
+}
+
+}  // namespace
+
+struct swe_sim {
+  swe_options o;
+  int nx, ny, W, H, N;
+  double dx, dy, eps4, R, dlam, dphi, totalArea;
+  std::vector<double> geom[SWE_GEOM_NROWS];
+  cudaStream_t st = nullptr;
+  double* d_b = nullptr;
+  double* d_A[3] = {nullptr, nullptr, nullptr};
+  double* d_B[3] = {nullptr, nullptr, nullptr};
+  double* d_h0[3] = {nullptr, nullptr, nullptr};
+  double* d_res[4] = {nullptr, nullptr, nullptr, nullptr};
+  double* d_nfield = nullptr;
+  double* d_geom = nullptr;
+  double* d_part = nullptr;
+  double* d_rows = nullptr;
+  double* d_sponge = nullptr;
+  swe::Control* d_ctl = nullptr;
+  int bc[4];
+  int fl_kind[4] = {0, 0, 0, 0};
+  double fl_eta[4] = {0, 0, 0, 0}, fl_u[4] = {0, 0, 0, 0};
+  int sponge_side = 1, sponge_width = 0;
+  double sponge_ref = 0;
+  bool keep_h0 = false;
+  bool cfl_valid = false;
+  double t = 0, steps = 0;        // host mirror of the device clock
+  bool clock_valid = true;
+  dim3 grid;
+  int nblocks = 0;
+  int part_cap = 0;
+  // device-resident loop graph
+  cudaGraphExec_t gexec = nullptr;
+  int g_steps = 0, g_mode = -1;
+  double g_dt = 0, g_tend = 0;
+  unsigned long long g_version = 0, version = 1;
+};
+
+namespace {
+
+void cartesian_geometry(swe_sim* s) {            // src/geometry.mjs:163-176
+  s->R = INFINITY; s->dlam = 0; s->dphi = 0;
+  s->totalArea = s->nx * s->dx * s->ny * s->dy;
+  for (int j = 0; j < s->H; j++) {
+    s->geom[SWE_GEOM_DXROW][j] = s->dx;
+    s->geom[SWE_GEOM_DYROWN][j] = s->dy;
+    s->geom[SWE_GEOM_DYROWS][j] = s->dy;
+    s->geom[SWE_GEOM_DYCFL][j] = s->dy;
+    s->geom[SWE_GEOM_BEDPHI][j] = s->dy;
+    s->geom[SWE_GEOM_AREA][j] = s->dx * s->dy;
+    s->geom[SWE_GEOM_LX][j] = s->dy;
+    s->geom[SWE_GEOM_LYN][j] = s->dx;
+    s->geom[SWE_GEOM_LYS][j] = s->dx;
+    s->geom[SWE_GEOM_FROW][j] = s->o.coriolis;
+  }
+}
+
+int spherical_geometry(swe_sim* s) {             // src/geometry.mjs:190-299
+  const int nx = s->nx, ny = s->ny;
+  const double R = s->o.R, lat0 = s->o.lat0, lat1 = s->o.lat1, omega = s->o.omega;
+  char buf[256];
+  if (!(lat1 > lat0)) {
+    std::snprintf(buf, sizeof buf, "lat1 (%.17g) must exceed lat0 (%.17g)", lat1, lat0);
+    return fail(SWE_EINVAL, buf);
+  }
+  if (lat0 < -90 || lat1 > 90) {
+    std::snprintf(buf, sizeof buf, "latitudes must lie in [-90, 90]; got %.17g..%.17g", lat0, lat1);
+    return fail(SWE_EINVAL, buf);
+  }
+  const bool touches_pole = lat0 <= -90 + 1e-12 || lat1 >= 90 - 1e-12;
+  if (touches_pole && nx % 2 != 0) {
+    std::snprintf(buf, sizeof buf,
+                  "nx must be even when the domain reaches a pole (got %d): a ghost row beyond the "
+                  "pole is the row half a turn away in longitude.", nx);
+    return fail(SWE_EINVAL, buf);
+  }
+  const double dlam = 2 * PI / nx;
+  const double p0 = lat0 * PI / 180, p1 = lat1 * PI / 180;
+  const double dphi = (p1 - p0) / ny;
+  s->R = R; s->dlam = dlam; s->dphi = dphi;
+  const double gdy = R * dphi;
+  s->dy = gdy;
+  s->totalArea = 2 * PI * R * R * (std::sin(p1) - std::sin(p0));
+  for (int j = 0; j < s->H; j++) {
+    const int jj = j - 2;
+    // face latitudes; the domain edges are pinned exactly (src/geometry.mjs:216)
+    const double rawS = jj == 0 ? p0 : jj == ny ? p1 : p0 + jj * dphi;
+    const double rawN = jj + 1 == 0 ? p0 : jj + 1 == ny ? p1 : p0 + (jj + 1) * dphi;
+    const double pS = clamp_lat(rawS), pN = clamp_lat(rawN);
+    const double pC = 0.5 * (pS + pN);
+    const double half = 0.5 * (pN - pS);
+    const double lyS = R * dlam * cos_lat(pS);
+    const double lyN = R * dlam * cos_lat(pN);
+    const double lx = R * dphi;
+    double A = 2 * R * R * dlam * cos_lat(pC) * std::sin(half);
+    if (!(A > 0)) {
+      const double rS = reflect_lat(rawS), rN = reflect_lat(rawN);
+      A = std::fabs(2 * R * R * dlam * cos_lat(0.5 * (rS + rN)) * std::sin(0.5 * (rN - rS)));
+    }
+    s->geom[SWE_GEOM_PHIC][j] = pC;
+    s->geom[SWE_GEOM_LYS][j] = lyS;
+    s->geom[SWE_GEOM_LYN][j] = lyN;
+    s->geom[SWE_GEOM_LX][j] = lx;
+    s->geom[SWE_GEOM_AREA][j] = A;
+    s->geom[SWE_GEOM_DXROW][j] = A / lx;
+    const double dN = lyN > 0 ? A / lyN : INFINITY;
+    const double dS = lyS > 0 ? A / lyS : INFINITY;
+    s->geom[SWE_GEOM_DYROWN][j] = dN;
+    s->geom[SWE_GEOM_DYROWS][j] = dS;
+    s->geom[SWE_GEOM_DYCFL][j] = js_min(js_min(dN, dS), gdy);
+    s->geom[SWE_GEOM_BEDPHI][j] = (lyN + lyS) > 0 ? 2 * A / (lyN + lyS) : INFINITY;
+    s->geom[SWE_GEOM_TANPHI][j] = std::tan(pC);
+    s->geom[SWE_GEOM_FROW][j] = 2 * omega * std::sin(pC);
+    s->geom[SWE_GEOM_GEOCOEF][j] = (lyN - lyS) / (4 * A);
+  }
+  for (int j = 0; j < s->H; j++) {
+    const double a = s->geom[SWE_GEOM_AREA][j];
+    if (!(a > 0) || !std::isfinite(a)) {
+      std::snprintf(buf, sizeof buf, "row %d: area %.17g", j, a);
+      return fail(SWE_EINVAL, buf);
+    }
+    if (!(s->geom[SWE_GEOM_LYN][j] >= 0) || !(s->geom[SWE_GEOM_LYS][j] >= 0)) {
+      std::snprintf(buf, sizeof buf, "row %d: negative face length", j);
+      return fail(SWE_EINVAL, buf);
+    }
+  }
+  return SWE_OK;
+}
+
+swe::Metric metric(const swe_sim* s) {
+  swe::Metric m;
+  const double* g = s->d_geom;
+  const int H = s->H;
+  m.dxRow = g + SWE_GEOM_DXROW * H; m.dyRowN = g + SWE_GEOM_DYROWN * H;
+  m.dyRowS = g + SWE_GEOM_DYROWS * H; m.dyCFL = g + SWE_GEOM_DYCFL * H;
+  m.bedPhi = g + SWE_GEOM_BEDPHI * H; m.geoCoef = g + SWE_GEOM_GEOCOEF * H;
+  m.fRow = g + SWE_GEOM_FROW * H; m.tanPhi = g + SWE_GEOM_TANPHI * H;
+  m.R = s->R;
+  return m;
+}
+
+// StageArgs reading `in` and writing `out`.
+swe::StageArgs stage_args(const swe_sim* s, double* const* in, double* const* out) {
+  swe::StageArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.W = s->W; a.H = s->H; a.nx = s->nx; a.ny = s->ny;
+  a.b = s->d_b;
+  a.h = in[0]; a.hu = in[1]; a.hv = in[2];
+  if (out) { a.oh = out[0]; a.ohu = out[1]; a.ohv = out[2]; }
+  a.m = metric(s);
+  a.minDepth = s->o.min_depth; a.eps4 = s->eps4; a.coriolis = s->o.coriolis;
+  a.sph = s->o.sphere; a.order = s->o.order; a.lim = s->o.limiter;
+  a.manning = s->o.manning; a.nfield = s->d_nfield;
+  a.sponge_side = s->sponge_side; a.sponge_width = s->sponge_width;
+  a.sponge_str = s->d_sponge; a.sponge_ref = s->sponge_ref;
+  a.part_max = s->d_part; a.part_fl1 = s->d_part + s->part_cap; a.part_fl2 = s->d_part + 2 * s->part_cap;
+  a.nblocks = s->nblocks;
+  return a;
+}
+
+swe::BCArgs bc_args(const swe_sim* s, double* const* f) {
+  swe::BCArgs a;
+  a.nx = s->nx; a.ny = s->ny; a.W = s->W; a.H = s->H;
+  for (int q = 0; q < 4; q++) a.kind[q] = s->bc[q];
+  a.minDepth = s->o.min_depth; a.eps4 = s->eps4;
+  a.b = s->d_b; a.h = f[0]; a.hu = f[1]; a.hv = f[2];
+  return a;
+}
+
+swe::PrepArgs prep_args(const swe_sim* s, int mode, double dt, double t_end) {
+  swe::PrepArgs p;
+  p.mode = mode; p.dt_host = dt; p.cfl = s->o.cfl; p.t_end = t_end;
+  for (int q = 0; q < 4; q++) { p.fl_kind[q] = s->fl_kind[q]; p.fl_eta[q] = s->fl_eta[q]; p.fl_u[q] = s->fl_u[q]; }
+  return p;
+}
+
+int bc_blocks(const swe_sim* s) { return (4 * s->ny + 4 * (s->nx + 4) + 255) / 256; }
+
+int launch_bc(swe_sim* s, double* const* f, int respect_stop) {
+  swe::k_apply_bc<<<bc_blocks(s), 256, 0, s->st>>>(bc_args(s, f), s->d_ctl, respect_stop);
+  CU(cudaGetLastError());
+  return SWE_OK;
+}
+
+// One SSP-RK2 step on the device; `mode`/`dt`/`t_end` as k_prepare.
+int enqueue_step(swe_sim* s, int mode, double dt, double t_end) {
+  swe::k_prepare<<<1, 32, 0, s->st>>>(s->d_ctl, prep_args(s, mode, dt, t_end));
+  CU(cudaGetLastError());
+  int rc = launch_bc(s, s->d_A, 0);
+  if (rc) return rc;
+  swe::StageArgs a1 = stage_args(s, s->d_A, s->d_B);
+  swe::k_stage<1><<<s->grid, swe::BX, 0, s->st>>>(a1, s->d_ctl);
+  CU(cudaGetLastError());
+  rc = launch_bc(s, s->d_B, 1);
+  if (rc) return rc;
+  swe::StageArgs a2 = stage_args(s, s->d_B, s->d_A);
+  if (s->keep_h0) { a2.h0c = s->d_h0[0]; a2.hu0c = s->d_h0[1]; a2.hv0c = s->d_h0[2]; }
+  swe::k_stage<2><<<s->grid, swe::BX, 0, s->st>>>(a2, s->d_ctl);
+  CU(cudaGetLastError());
+  return SWE_OK;
+}
+
+int ensure_cfl(swe_sim* s) {
+  if (s->cfl_valid) return SWE_OK;
+  swe::StageArgs a = stage_args(s, s->d_A, nullptr);
+  const int nb = std::min(s->part_cap, std::max(1, (s->nx * s->ny + 255) / 256));
+  swe::k_cfl_rate<<<nb, swe::BX, 0, s->st>>>(a, s->d_ctl, s->d_part);
+  CU(cudaGetLastError());
+  s->cfl_valid = true;
+  return SWE_OK;
+}
+
+int read_ctl(swe_sim* s, swe::Control* out) {
+  CU(cudaMemcpyAsync(out, s->d_ctl, sizeof(swe::Control), cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int sync_clock(swe_sim* s) {
+  if (s->clock_valid) return SWE_OK;
+  swe::Control c;
+  int rc = read_ctl(s, &c);
+  if (rc) return rc;
+  s->t = c.t; s->steps = c.steps;
+  s->clock_valid = true;
+  return SWE_OK;
+}
+
+double* field_ptr(swe_sim* s, int f) {
+  switch (f) {
+    case SWE_FIELD_B: return s->d_b;
+    case SWE_FIELD_H: return s->d_A[0];
+    case SWE_FIELD_HU: return s->d_A[1];
+    case SWE_FIELD_HV: return s->d_A[2];
+    case SWE_FIELD_H0: return s->d_h0[0];
+    case SWE_FIELD_HU0: return s->d_h0[1];
+    case SWE_FIELD_HV0: return s->d_h0[2];
+    case SWE_FIELD_RH: return s->d_res[0];
+    case SWE_FIELD_RHU: return s->d_res[1];
+    case SWE_FIELD_RHV: return s->d_res[2];
+    case SWE_FIELD_THETA: return s->d_res[3];
+    case SWE_FIELD_MANNING: return s->d_nfield;
+    default: return nullptr;
+  }
+}
+
+int upload_geom(swe_sim* s) {
+  for (int r = 0; r < SWE_GEOM_NROWS; r++)
+    CU(cudaMemcpyAsync(s->d_geom + (size_t)r * s->H, s->geom[r].data(), sizeof(double) * s->H,
+                       cudaMemcpyHostToDevice, s->st));
+  return SWE_OK;
+}
+
+void free_all(swe_sim* s) {
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  double** ptrs[] = {&s->d_b, &s->d_A[0], &s->d_A[1], &s->d_A[2], &s->d_B[0], &s->d_B[1], &s->d_B[2],
+                     &s->d_h0[0], &s->d_h0[1], &s->d_h0[2], &s->d_res[0], &s->d_res[1], &s->d_res[2],
+                     &s->d_res[3], &s->d_nfield, &s->d_geom, &s->d_part, &s->d_rows, &s->d_sponge};
+  for (double** p : ptrs) if (*p) { cudaFree(*p); *p = nullptr; }
+  if (s->d_ctl) cudaFree(s->d_ctl);
+  if (s->st) cudaStreamDestroy(s->st);
+}
+
+int choose_rows_per_cta(const swe_sim* s) {
+  const char* env = std::getenv("SWE_B200_ROWS_PER_CTA");
+  if (env) { const int v = std::atoi(env); if (v >= 4) return v; }
+  return 32;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* swe_last_error(void) { return g_err.c_str(); }
+
+int swe_set_device(int ordinal) {
+  CU(cudaSetDevice(ordinal));
+  return SWE_OK;
+}
+
+int swe_options_init(swe_options* o) {
+  if (!o) return fail(SWE_EINVAL, "null options");
+  std::memset(o, 0, sizeof *o);
+  o->dx = 1; o->dy = 1;
+  o->manning = 0.025; o->min_depth = 1e-3; o->cfl = 0.45; o->coriolis = 0;
+  o->order = 2; o->limiter = SWE_LIMITER_MC; o->sphere = 0;
+  o->R = 6371e3; o->lat0 = -90; o->lat1 = 90; o->omega = 0;
+  return SWE_OK;
+}
+
+int swe_create(const swe_options* o, const double* b, const double* h, swe_sim** out) {
+  if (!out) return fail(SWE_EINVAL, "null output handle");
+  *out = nullptr;
+  if (!o) return fail(SWE_EINVAL, "null options");
+  if (o->nx < 1 || o->ny < 1) return fail(SWE_EINVAL, "nx and ny must be >= 1");
+  if (o->limiter < 0 || o->limiter > 2)
+    return fail(SWE_EINVAL, "unknown limiter; have minmod,mc,central");   // src/swe.mjs:195
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+    return fail(SWE_ECUDA, "no CUDA device is available; this library has no CPU path");
+  swe_sim* s = new swe_sim();
+  s->o = *o;
+  s->nx = o->nx; s->ny = o->ny; s->W = o->nx + 4; s->H = o->ny + 4; s->N = s->W * s->H;
+  s->dx = o->dx; s->dy = o->dy;
+  s->eps4 = std::pow(js_max(o->min_depth, 1e-12), 4.0);   // src/swe.mjs:190
+  for (int r = 0; r < SWE_GEOM_NROWS; r++) s->geom[r].assign(s->H, 0.0);
+  if (o->sphere) {
+    const int rc = spherical_geometry(s);
+    if (rc) { delete s; return rc; }
+    s->dx = NAN;
+  } else {
+    cartesian_geometry(s);
+  }
+  // src/swe.mjs:239-241
+  s->bc[0] = s->bc[1] = o->sphere ? SWE_BC_PERIODIC : SWE_BC_REFLECT;
+  s->bc[2] = s->bc[3] = SWE_BC_REFLECT;
+
+  const int gx = (s->W + swe::SX - 1) / swe::SX;
+  const int ry = choose_rows_per_cta(s);
+  const int gy = (s->H + ry - 1) / ry;
+  s->grid = dim3(gx, gy, 1);
+  s->nblocks = gx * gy;
+  s->part_cap = std::max(s->nblocks, 1024);
+
+  auto bail = [&](int rc) { free_all(s); delete s; return rc; };
+  const size_t nb = sizeof(double) * (size_t)s->N;
+#define CUB(call)                                                                           \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) return bail(fail(SWE_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_))); \
+  } while (0)
+  CUB(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  CUB(cudaMalloc(&s->d_b, nb));
+  for (int q = 0; q < 3; q++) { CUB(cudaMalloc(&s->d_A[q], nb)); CUB(cudaMalloc(&s->d_B[q], nb)); }
+  CUB(cudaMalloc(&s->d_geom, sizeof(double) * SWE_GEOM_NROWS * s->H));
+  CUB(cudaMalloc(&s->d_part, sizeof(double) * 3 * s->part_cap));
+  CUB(cudaMalloc(&s->d_rows, sizeof(double) * std::max(1, s->ny)));
+  CUB(cudaMalloc(&s->d_ctl, sizeof(swe::Control)));
+  CUB(cudaMemsetAsync(s->d_ctl, 0, sizeof(swe::Control), s->st));
+  CUB(cudaMemsetAsync(s->d_part, 0, sizeof(double) * 3 * s->part_cap, s->st));
+  for (int q = 0; q < 3; q++) {
+    CUB(cudaMemsetAsync(s->d_A[q], 0, nb, s->st));
+    CUB(cudaMemsetAsync(s->d_B[q], 0, nb, s->st));
+  }
+  if (b) CUB(cudaMemcpyAsync(s->d_b, b, nb, cudaMemcpyHostToDevice, s->st));
+  else CUB(cudaMemsetAsync(s->d_b, 0, nb, s->st));
+  if (h) CUB(cudaMemcpyAsync(s->d_A[0], h, nb, cudaMemcpyHostToDevice, s->st));
+  if (upload_geom(s)) return bail(SWE_ECUDA);
+  CUB(cudaStreamSynchronize(s->st));
+#undef CUB
+  *out = s;
+  return SWE_OK;
+}
+
+int swe_destroy(swe_sim* s) {
+  if (!s) return SWE_OK;
+  if (s->st) cudaStreamSynchronize(s->st);
+  free_all(s);
+  delete s;
+  return SWE_OK;
+}
+
+int swe_get_dims(swe_sim* s, int* d) {
+  if (!s || !d) return fail(SWE_EINVAL, "null argument");
+  d[0] = s->W; d[1] = s->H; d[2] = s->nx; d[3] = s->ny;
+  return SWE_OK;
+}
+
+int swe_get_field(swe_sim* s, int field, double* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  if (field < 0 || field > SWE_FIELD_MANNING) return fail(SWE_EINVAL, "unknown field id");
+  const size_t nb = sizeof(double) * (size_t)s->N;
+  double* p = field_ptr(s, field);
+  if (!p) {
+    if (field == SWE_FIELD_MANNING) return fail(SWE_EINVAL, "no Manning field is set");
+    std::memset(out, 0, nb);          // never written yet: a fresh Float64Array is zeros
+    CU(cudaStreamSynchronize(s->st));
+    return SWE_OK;
+  }
+  CU(cudaMemcpyAsync(out, p, nb, cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_set_field(swe_sim* s, int field, const double* in) {
+  if (!s || !in) return fail(SWE_EINVAL, "null argument");
+  if (field != SWE_FIELD_B && field != SWE_FIELD_H && field != SWE_FIELD_HU && field != SWE_FIELD_HV)
+    return fail(SWE_EINVAL, "only b, h, hu, hv are writable (use swe_set_manning_field for n)");
+  const size_t nb = sizeof(double) * (size_t)s->N;
+  CU(cudaMemcpyAsync(field_ptr(s, field), in, nb, cudaMemcpyHostToDevice, s->st));
+  s->cfl_valid = false;
+  return SWE_OK;
+}
+
+int swe_get_geom(swe_sim* s, int row, double* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  if (row < 0 || row >= SWE_GEOM_NROWS) return fail(SWE_EINVAL, "unknown metric row id");
+  std::memcpy(out, s->geom[row].data(), sizeof(double) * s->H);
+  return SWE_OK;
+}
+
+int swe_set_geom(swe_sim* s, int row, const double* in) {
+  if (!s || !in) return fail(SWE_EINVAL, "null argument");
+  if (row < 0 || row >= SWE_GEOM_NROWS) return fail(SWE_EINVAL, "unknown metric row id");
+  std::memcpy(s->geom[row].data(), in, sizeof(double) * s->H);
+  CU(cudaMemcpyAsync(s->d_geom + (size_t)row * s->H, s->geom[row].data(), sizeof(double) * s->H,
+                     cudaMemcpyHostToDevice, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  s->cfl_valid = false;
+  return SWE_OK;
+}
+
+int swe_get_scalar(swe_sim* s, int which, double* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  switch (which) {
+    case SWE_SCALAR_DX: *out = s->dx; return SWE_OK;
+    case SWE_SCALAR_DY: *out = s->dy; return SWE_OK;
+    case SWE_SCALAR_R: *out = s->R; return SWE_OK;
+    case SWE_SCALAR_DLAM: *out = s->dlam; return SWE_OK;
+    case SWE_SCALAR_DPHI: *out = s->dphi; return SWE_OK;
+    case SWE_SCALAR_TOTAL_AREA: *out = s->totalArea; return SWE_OK;
+    case SWE_SCALAR_EPS4: *out = s->eps4; return SWE_OK;
+    case SWE_SCALAR_T: { int rc = sync_clock(s); if (rc) return rc; *out = s->t; return SWE_OK; }
+    case SWE_SCALAR_STEPS: { int rc = sync_clock(s); if (rc) return rc; *out = s->steps; return SWE_OK; }
+    case SWE_SCALAR_MASS_FLOORED: {
+      swe::Control c; int rc = read_ctl(s, &c); if (rc) return rc;
+      *out = c.mass_floored; return SWE_OK;
+    }
+    default: return fail(SWE_EINVAL, "unknown scalar id");
+  }
+}
+
+int swe_set_scalar(swe_sim* s, int which, double v) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  int rc = sync_clock(s);
+  if (rc) return rc;
+  size_t off;
+  if (which == SWE_SCALAR_T) { s->t = v; off = offsetof(swe::Control, t); }
+  else if (which == SWE_SCALAR_STEPS) { s->steps = v; off = offsetof(swe::Control, steps); }
+  else return fail(SWE_EINVAL, "only t and steps are settable");
+  CU(cudaMemcpyAsync((char*)s->d_ctl + off, &v, sizeof(double), cudaMemcpyHostToDevice, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_set_boundary(swe_sim* s, int side, int kind) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (side < 0 || side > 3) return fail(SWE_EINVAL, "side must be 0..3 (west, east, south, north)");
+  if (kind < 0 || kind > 3) return fail(SWE_EINVAL, "unknown boundary kind");
+  s->bc[side] = kind;
+  if (kind != SWE_BC_FLATHER) s->fl_kind[side] = 0;
+  s->version++;
+  return SWE_OK;
+}
+
+int swe_set_flather_values(swe_sim* s, int side, double eta_ext, double u_ext) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (side < 0 || side > 3) return fail(SWE_EINVAL, "side must be 0..3");
+  s->bc[side] = SWE_BC_FLATHER;
+  s->fl_kind[side] = 0;
+  s->fl_eta[side] = eta_ext; s->fl_u[side] = u_ext;
+  s->version++;
+  return SWE_OK;
+}
+
+int swe_set_flather_tide(swe_sim* s, int side, double msl, int n, const double* amp,
+                         const double* omega, const double* phase_deg, double u_coef) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (side < 0 || side > 3) return fail(SWE_EINVAL, "side must be 0..3");
+  if (n < 0 || n > swe::MAX_TIDE) return fail(SWE_EINVAL, "tide tables hold at most 16 constituents");
+  if (n > 0 && (!amp || !omega || !phase_deg)) return fail(SWE_EINVAL, "null tide table");
+  swe::Control c;
+  int rc = read_ctl(s, &c);
+  if (rc) return rc;
+  c.tide_n[side] = n; c.tide_msl[side] = msl; c.tide_ucoef[side] = u_coef;
+  for (int q = 0; q < n; q++) {
+    c.tide_amp[side][q] = amp[q]; c.tide_omega[side][q] = omega[q]; c.tide_phase[side][q] = phase_deg[q];
+  }
+  CU(cudaMemcpyAsync(s->d_ctl, &c, sizeof c, cudaMemcpyHostToDevice, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  s->bc[side] = SWE_BC_FLATHER;
+  s->fl_kind[side] = 1;
+  s->version++;
+  return SWE_OK;
+}
+
+int swe_set_manning_field(swe_sim* s, const double* n) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  s->version++;
+  s->cfl_valid = false;
+  if (!n) {
+    if (s->d_nfield) { cudaStreamSynchronize(s->st); cudaFree(s->d_nfield); s->d_nfield = nullptr; }
+    return SWE_OK;
+  }
+  for (int k = 0; k < s->N; k++) {                   // src/swe.mjs:723-725
+    const double v = n[k];
+    if (!(v >= 0) || !std::isfinite(v)) {
+      char buf[200];
+      std::snprintf(buf, sizeof buf, "setManningField: n = %.17g at cell %d; Manning n must be finite and >= 0", v, k);
+      return fail(SWE_EINVAL, buf);
+    }
+  }
+  if (!s->d_nfield) CU(cudaMalloc(&s->d_nfield, sizeof(double) * s->N));
+  CU(cudaMemcpyAsync(s->d_nfield, n, sizeof(double) * s->N, cudaMemcpyHostToDevice, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_set_sponge(swe_sim* s, int side, int width, double strength, double eta_ref) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (side < 0 || side > 3) return fail(SWE_EINVAL, "side must be 0..3");
+  if (width < 0) return fail(SWE_EINVAL, "sponge width must be >= 0");
+  // per-distance strength, src/swe.mjs:1182-1183
+  std::vector<double> str(std::max(1, width));
+  for (int d = 0; d < width; d++) {
+    const double c = std::cos(0.5 * PI * d / width);
+    str[d] = strength * (c * c);
+  }
+  if (s->d_sponge) { cudaStreamSynchronize(s->st); cudaFree(s->d_sponge); s->d_sponge = nullptr; }
+  CU(cudaMalloc(&s->d_sponge, sizeof(double) * str.size()));
+  CU(cudaMemcpyAsync(s->d_sponge, str.data(), sizeof(double) * str.size(), cudaMemcpyHostToDevice, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  s->sponge_side = side; s->sponge_width = width; s->sponge_ref = eta_ref;
+  s->version++;
+  return SWE_OK;
+}
+
+int swe_clear_sponge(swe_sim* s) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  s->sponge_width = 0;
+  s->version++;
+  return SWE_OK;
+}
+
+int swe_set_keep_h0(swe_sim* s, int on) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (on && !s->d_h0[0]) {
+    for (int q = 0; q < 3; q++) {
+      CU(cudaMalloc(&s->d_h0[q], sizeof(double) * s->N));
+      CU(cudaMemsetAsync(s->d_h0[q], 0, sizeof(double) * s->N, s->st));
+    }
+  }
+  s->keep_h0 = on != 0;
+  s->version++;
+  return SWE_OK;
+}
+
+int swe_apply_bc(swe_sim* s) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  swe::k_prepare<<<1, 32, 0, s->st>>>(s->d_ctl, prep_args(s, 0, 0, INFINITY));
+  CU(cudaGetLastError());
+  const int rc = launch_bc(s, s->d_A, 0);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_residual(swe_sim* s, double dt) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (!s->d_res[0])
+    for (int q = 0; q < 4; q++) {
+      CU(cudaMalloc(&s->d_res[q], sizeof(double) * s->N));
+      CU(cudaMemsetAsync(s->d_res[q], 0, sizeof(double) * s->N, s->st));
+    }
+  swe::k_prepare<<<1, 32, 0, s->st>>>(s->d_ctl, prep_args(s, 0, dt, INFINITY));
+  CU(cudaGetLastError());
+  swe::StageArgs a = stage_args(s, s->d_A, nullptr);
+  a.rh = s->d_res[0]; a.rhu = s->d_res[1]; a.rhv = s->d_res[2]; a.theta = s->d_res[3];
+  swe::k_stage<0><<<s->grid, swe::BX, 0, s->st>>>(a, s->d_ctl);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_max_dt(swe_sim* s, double* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  int rc = ensure_cfl(s);
+  if (rc) return rc;
+  swe::Control c;
+  rc = read_ctl(s, &c);
+  if (rc) return rc;
+  *out = c.next_max > 0 ? s->o.cfl / c.next_max : INFINITY;
+  return SWE_OK;
+}
+
+int swe_apply_friction(swe_sim* s, double dt) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  swe::StageArgs a = stage_args(s, s->d_A, s->d_A);
+  swe::k_friction<<<std::max(1, std::min(4096, (s->nx * s->ny + 255) / 256)), 256, 0, s->st>>>(a, dt);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(s->st));
+  s->cfl_valid = false;
+  return SWE_OK;
+}
+
+int swe_dry_clean(swe_sim* s, double* added) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  swe::StageArgs a = stage_args(s, s->d_A, s->d_A);
+  swe::k_dry_clean<<<1, 1, 0, s->st>>>(a, s->d_ctl);
+  CU(cudaGetLastError());
+  swe::Control c;
+  const int rc = read_ctl(s, &c);
+  if (rc) return rc;
+  if (added) *added = c.diag;
+  s->cfl_valid = false;
+  return SWE_OK;
+}
+
+int swe_step(swe_sim* s, double dt, double* taken) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (taken) *taken = 0;
+  int rc = sync_clock(s);
+  if (rc) return rc;
+  if (!(dt > 0) || !std::isfinite(dt)) {   // src/swe.mjs:783-784, after applyBC
+    swe::k_prepare<<<1, 32, 0, s->st>>>(s->d_ctl, prep_args(s, 0, 0, INFINITY));
+    CU(cudaGetLastError());
+    rc = launch_bc(s, s->d_A, 0);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(s->st));
+    return SWE_OK;
+  }
+  rc = enqueue_step(s, 0, dt, INFINITY);
+  if (rc) return rc;
+  s->t = s->t + dt;
+  s->steps = s->steps + 1;
+  s->cfl_valid = true;
+  if (taken) *taken = dt;
+  return SWE_OK;
+}
+
+int swe_step_auto(swe_sim* s, double* taken) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  double dt;
+  const int rc = swe_max_dt(s, &dt);
+  if (rc) return rc;
+  return swe_step(s, dt, taken);
+}
+
+int swe_run(swe_sim* s, int n, double dt_fixed, double t_end, int* done) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (done) *done = 0;
+  if (n <= 0) return SWE_OK;
+  int rc = sync_clock(s);
+  if (rc) return rc;
+  rc = ensure_cfl(s);
+  if (rc) return rc;
+  const double steps0 = s->steps;
+  const int mode = dt_fixed > 0 ? 2 : 3;
+  const double dtv = dt_fixed > 0 ? dt_fixed : 0;
+  const int chunk = std::min(n, 32);
+  if (!s->gexec || s->g_steps != chunk || s->g_mode != mode || s->g_dt != dtv || s->g_tend != t_end ||
+      s->g_version != s->version) {
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    cudaGraph_t graph;
+    CU(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+    for (int q = 0; q < chunk; q++) {
+      rc = enqueue_step(s, mode, dtv, t_end);
+      if (rc) { cudaStreamEndCapture(s->st, &graph); return rc; }
+    }
+    CU(cudaStreamEndCapture(s->st, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&s->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(SWE_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    s->g_steps = chunk; s->g_mode = mode; s->g_dt = dtv; s->g_tend = t_end; s->g_version = s->version;
+  }
+  int left = n;
+  while (left >= chunk) {
+    CU(cudaGraphLaunch(s->gexec, s->st));
+    left -= chunk;
+  }
+  for (int q = 0; q < left; q++) {
+    rc = enqueue_step(s, mode, dtv, t_end);
+    if (rc) return rc;
+  }
+  s->clock_valid = false;
+  s->cfl_valid = true;
+  rc = sync_clock(s);
+  if (rc) return rc;
+  if (done) *done = (int)(s->steps - steps0);
+  return SWE_OK;
+}
+
+static int finish_diag(swe_sim* s, double* out) {
+  swe::Control c;
+  const int rc = read_ctl(s, &c);
+  if (rc) return rc;
+  *out = c.diag;
+  return SWE_OK;
+}
+
+int swe_volume(swe_sim* s, double* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  swe::StageArgs a = stage_args(s, s->d_A, nullptr);
+  if (s->o.sphere) {
+    swe::k_row_sums<<<(s->ny + 127) / 128, 128, 0, s->st>>>(a, 0, s->d_rows);
+    CU(cudaGetLastError());
+  }
+  swe::k_finish_sum<<<1, 1, 0, s->st>>>(a, 0, s->d_rows, s->d_geom + SWE_GEOM_AREA * s->H, s->dx, s->dy, s->d_ctl);
+  CU(cudaGetLastError());
+  return finish_diag(s, out);
+}
+
+int swe_energy(swe_sim* s, double* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  swe::StageArgs a = stage_args(s, s->d_A, nullptr);
+  swe::k_row_sums<<<(s->ny + 127) / 128, 128, 0, s->st>>>(a, 1, s->d_rows);
+  CU(cudaGetLastError());
+  swe::k_finish_sum<<<1, 1, 0, s->st>>>(a, 1, s->d_rows, s->d_geom + SWE_GEOM_AREA * s->H, s->dx, s->dy, s->d_ctl);
+  CU(cudaGetLastError());
+  return finish_diag(s, out);
+}
+
+static int max_diag(swe_sim* s, int what, double ref, double* out) {
+  swe::StageArgs a = stage_args(s, s->d_A, nullptr);
+  const int total = what == 2 ? s->N : s->nx * s->ny;
+  const int nb = std::min(s->part_cap, std::max(1, (total + 255) / 256));
+  swe::k_max_diag<<<nb, swe::BX, 0, s->st>>>(a, what, ref, s->d_part, s->d_ctl);
+  CU(cudaGetLastError());
+  return finish_diag(s, out);
+}
+
+int swe_max_surface_deviation(swe_sim* s, double ref, double* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  return max_diag(s, 0, ref, out);
+}
+
+int swe_max_speed(swe_sim* s, double* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  return max_diag(s, 1, 0, out);
+}
+
+int swe_finite(swe_sim* s, int* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  double bad = 0;
+  const int rc = max_diag(s, 2, 0, &bad);
+  if (rc) return rc;
+  *out = bad == 0 ? 1 : 0;
+  return SWE_OK;
+}
+
+int swe_compute_geometry(const swe_options* o, double* rows, double* scalars) {
+  if (!o || !rows) return fail(SWE_EINVAL, "null argument");
+  if (o->nx < 1 || o->ny < 1) return fail(SWE_EINVAL, "nx and ny must be >= 1");
+  swe_sim tmp;
+  tmp.o = *o;
+  tmp.nx = o->nx; tmp.ny = o->ny; tmp.W = o->nx + 4; tmp.H = o->ny + 4; tmp.N = tmp.W * tmp.H;
+  tmp.dx = o->dx; tmp.dy = o->dy;
+  for (int r = 0; r < SWE_GEOM_NROWS; r++) tmp.geom[r].assign(tmp.H, 0.0);
+  if (o->sphere) {
+    const int rc = spherical_geometry(&tmp);
+    if (rc) return rc;
+    tmp.dx = NAN;
+  } else {
+    cartesian_geometry(&tmp);
+  }
+  for (int r = 0; r < SWE_GEOM_NROWS; r++)
+    std::memcpy(rows + (size_t)r * tmp.H, tmp.geom[r].data(), sizeof(double) * tmp.H);
+  if (scalars) {
+    scalars[SWE_SCALAR_DX] = tmp.dx; scalars[SWE_SCALAR_DY] = tmp.dy; scalars[SWE_SCALAR_R] = tmp.R;
+    scalars[SWE_SCALAR_DLAM] = tmp.dlam; scalars[SWE_SCALAR_DPHI] = tmp.dphi;
+    scalars[SWE_SCALAR_TOTAL_AREA] = tmp.totalArea;
+  }
+  return SWE_OK;
+}
+
+int swe_get_stream(swe_sim* s, void** stream) {
+  if (!s || !stream) return fail(SWE_EINVAL, "null argument");
+  *stream = (void*)s->st;
+  return SWE_OK;
+}
+
+int swe_step_timed(swe_sim* s, double dt, double* ms) {
+  if (!s || !ms) return fail(SWE_EINVAL, "null argument");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(SWE_EINVAL, "swe_step_timed needs a valid dt");
+  int rc = sync_clock(s);
+  if (rc) return rc;
+  cudaEvent_t ev[6];
+  for (int q = 0; q < 6; q++) CU(cudaEventCreate(&ev[q]));
+  CU(cudaEventRecord(ev[0], s->st));
+  swe::k_prepare<<<1, 32, 0, s->st>>>(s->d_ctl, prep_args(s, 0, dt, INFINITY));
+  CU(cudaEventRecord(ev[1], s->st));
+  rc = launch_bc(s, s->d_A, 0);
+  if (rc) return rc;
+  CU(cudaEventRecord(ev[2], s->st));
+  swe::k_stage<1><<<s->grid, swe::BX, 0, s->st>>>(stage_args(s, s->d_A, s->d_B), s->d_ctl);
+  CU(cudaEventRecord(ev[3], s->st));
+  rc = launch_bc(s, s->d_B, 1);
+  if (rc) return rc;
+  CU(cudaEventRecord(ev[4], s->st));
+  swe::StageArgs a2 = stage_args(s, s->d_B, s->d_A);
+  if (s->keep_h0) { a2.h0c = s->d_h0[0]; a2.hu0c = s->d_h0[1]; a2.hv0c = s->d_h0[2]; }
+  swe::k_stage<2><<<s->grid, swe::BX, 0, s->st>>>(a2, s->d_ctl);
+  CU(cudaEventRecord(ev[5], s->st));
+  CU(cudaEventSynchronize(ev[5]));
+  for (int q = 0; q < 5; q++) {
+    float f = 0;
+    CU(cudaEventElapsedTime(&f, ev[q], ev[q + 1]));
+    ms[q] = f;
+  }
+  for (int q = 0; q < 6; q++) cudaEventDestroy(ev[q]);
+  s->t = s->t + dt;
+  s->steps = s->steps + 1;
+  s->cfl_valid = true;
+  return SWE_OK;
+}
+
+int swe_get_launch_config(swe_sim* s, int* cfg) {
+  if (!s || !cfg) return fail(SWE_EINVAL, "null argument");
+  cfg[0] = (int)s->grid.x; cfg[1] = (int)s->grid.y; cfg[2] = swe::BX; cfg[3] = swe::SX;
+  cfg[4] = (s->H + (int)s->grid.y - 1) / (int)s->grid.y;
+  return SWE_OK;
+}
+
+int swe_synchronize(swe_sim* s) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_hllc_batch(int n, const double* in, double* out) {
+  if (n < 0 || (n > 0 && (!in || !out))) return fail(SWE_EINVAL, "bad arguments");
+  if (n == 0) return SWE_OK;
+  double *d_in = nullptr, *d_out = nullptr;
+  CU(cudaMalloc(&d_in, sizeof(double) * 7 * n));
+  cudaError_t e = cudaMalloc(&d_out, sizeof(double) * 3 * n);
+  if (e == cudaSuccess) e = cudaMemcpy(d_in, in, sizeof(double) * 7 * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    swe::k_hllc_batch<<<(n + 127) / 128, 128>>>(n, d_in, d_out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, d_out, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost);
+  cudaFree(d_in);
+  if (d_out) cudaFree(d_out);
+  if (e != cudaSuccess) return fail(SWE_ECUDA, std::string("hllc batch: ") + cudaGetErrorString(e));
+  return SWE_OK;
+}
+
+int swe_vel_batch(swe_sim* s, int n, const double* hq, const double* h, double* out) {
+  if (!s || n < 0 || (n > 0 && (!hq || !h || !out))) return fail(SWE_EINVAL, "bad arguments");
+  if (n == 0) return SWE_OK;
+  double* d = nullptr;
+  CU(cudaMalloc(&d, sizeof(double) * 3 * n));
+  cudaError_t e = cudaMemcpyAsync(d, hq, sizeof(double) * n, cudaMemcpyHostToDevice, s->st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d + n, h, sizeof(double) * n, cudaMemcpyHostToDevice, s->st);
+  if (e == cudaSuccess) {
+    swe::k_vel_batch<<<(n + 127) / 128, 128, 0, s->st>>>(n, d, d + n, s->eps4, d + 2 * n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(SWE_ECUDA, std::string("vel batch: ") + cudaGetErrorString(e));
+  return SWE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,79 @@
+"""Seeded synthetic inputs with the shapes of the benchmark configurations.
+
+No dataset exists for this path; every benchmark input is generated here
+from a seed, so the same arrays are produced wherever it runs.
+"""
+import math
+
+import numpy as np
+
+
+def uniform_noise(seed, shape, lo, hi):
+    """U(lo, hi) per cell from a counter-based hash (splitmix64 of seed, k)."""
+    n = int(np.prod(shape))
+    k = np.arange(n, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = k + np.uint64(seed) * np.uint64(0x100000001B3) + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) / float(1 << 53)
+    return (lo + (hi - lo) * u).reshape(shape)
+
+
+def _centres(nx, ny, dx, dy=None):
+    dy = dx if dy is None else dy
+    x = (np.arange(nx + 4) - 2 + 0.5) * dx
+    y = (np.arange(ny + 4) - 2 + 0.5) * dy
+    return np.meshgrid(x, y)
+
+
+def bump_bed(nx, ny, dx, seed=1, height=1.5, sigma=40.0, rough=0.2):
+    """Gaussian bump (height 1.5 m, sigma 40 m) at the domain centre plus
+    seeded uniform roughness +/- 0.2 m, over the padded grid."""
+    X, Y = _centres(nx, ny, dx)
+    cx, cy = nx * dx / 2, ny * dx / 2
+    b = height * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * sigma * sigma))
+    return b + uniform_noise(seed, X.shape, -rough, rough)
+
+
+def beach_bed(nx, ny, dx, seed=2):
+    """Sloping beach 1:50 plus smooth noise of amplitude 0.3 m:
+    b = -10 + x/50 + 0.3 s(x, y), s the mean of 8 seeded plane sinusoids with
+    wavelengths in [100, 1000] m (|s| <= 1)."""
+    X, Y = _centres(nx, ny, dx)
+    rng = np.random.default_rng(seed)
+    s = np.zeros_like(X)
+    for _ in range(8):
+        lam = rng.uniform(100, 1000)
+        ang = rng.uniform(0, 2 * math.pi)
+        ph = rng.uniform(0, 2 * math.pi)
+        kx, ky = 2 * math.pi / lam * math.cos(ang), 2 * math.pi / lam * math.sin(ang)
+        s += np.sin(kx * X + ky * Y + ph)
+    s /= 8
+    return -10 + X / 50 + 0.3 * s
+
+
+def _jmax0(d):
+    return np.where(d > 0, d, np.where(np.isnan(d), d, 0.0))
+
+
+def beach_dam_break(nx=2048, ny=2048, dx=2.0, seed=2, eta_left=5.0, x_dam=500.0):
+    """The 2048 x 2048 wet/dry workload: dam break over the sloping beach,
+    water at eta = 5 m for x < 500 m, dry land beyond (eta = 0 there, and the
+    bed rises above 0 at x ~ 500 m).  Returns (b, h) over the padded grid.
+    Manning n = 0.03, Flather(0, 0) on the west side, walls elsewhere."""
+    b = beach_bed(nx, ny, dx, seed)
+    X, _ = _centres(nx, ny, dx)
+    eta = np.where(X < x_dam, eta_left, 0.0)
+    return b, _jmax0(eta - b)
+
+
+def bump_dam_break(nx=256, ny=256, dx=5.0, seed=1, still=False):
+    """The plain 256 x 256 workload: bump + roughness under still water at
+    eta = 2 m, or the dam-break variant (2 m left half, 0.5 m right half).
+    Returns (b, eta0) over the padded grid."""
+    b = bump_bed(nx, ny, dx, seed)
+    X, _ = _centres(nx, ny, dx)
+    eta = np.full_like(X, 2.0) if still else np.where(X < nx * dx / 2, 2.0, 0.5)
+    return b, eta
