@@ -48,7 +48,12 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    return p.parse_args()
+    p.add_argument("--nx", type=int, default=2048, help="grid size (the workload is 2048x2048)")
+    p.add_argument("--ny", type=int, default=2048)
+    a = p.parse_args()
+    global NX, NY
+    NX, NY = a.nx, a.ny
+    return a
 
 
 def dist_env():

@@ -9,6 +9,8 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 import __graft_entry__  # noqa: E402
 
+__graft_entry__.load_package()   # registers water_simulator_b200 for module-level imports
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
