@@ -269,9 +269,8 @@ __global__ void __launch_bounds__(BX, 3) k_stage(StageArgs a, Control* ctl) {
   double b_m2 = 0, h_m2 = 0, U_m2 = 0, V_m2 = 0;     // row r-2
   double U_m3 = 0;                                   // row r-3
   double ysE = 0, ysB = 0, ysU = 0, ysV = 0;         // y slopes of row r-2
-  double tb0_m1 = 0, tb1_m1 = 0, tg_m1 = 0;          // bed terms of rows r-1.. r-3
-  double tb0_m2 = 0, tb1_m2 = 0, tg_m2 = 0;
-  double tb0_m3 = 0, tb1_m3 = 0, tg_m3 = 0;
+  double tb0_m2 = 0, tb1_m2 = 0, tg_m2 = 0;          // bed terms of row r-2 (computed last row)
+  double tb0_m3 = 0, tb1_m3 = 0, tg_m3 = 0;          // bed terms of row r-3
   Face fy1 = {0, 0, 0, 0, 0}, fy2 = {0, 0, 0, 0, 0}; // y faces (r-3|r-2), (r-4|r-3)
   double th_m3 = 1, th_m4 = 1;
   double locMax = 0, locFl = 0;
@@ -494,9 +493,8 @@ __global__ void __launch_bounds__(BX, 3) k_stage(StageArgs a, Control* ctl) {
     b_m2 = b_m1; h_m2 = h_m1; U_m2 = U_m1; V_m2 = V_m1;
     b_m1 = b_c; h_m1 = h_c; U_m1 = U_c; V_m1 = V_c;
     ysE = nsE; ysB = nsB; ysU = nsU; ysV = nsV;
-    tb0_m3 = tb0_m2; tb1_m3 = tb1_m2; tg_m3 = tg_m2;
-    tb0_m2 = tb0_m1; tb1_m2 = tb1_m1; tg_m2 = tg_m1;
-    tb0_m1 = tb0; tb1_m1 = tb1; tg_m1 = tg;
+    tb0_m3 = tb0_m2; tb1_m3 = tb1_m2; tg_m3 = tg_m2;   // bed terms computed at S2 are row r-1's
+    tb0_m2 = tb0; tb1_m2 = tb1; tg_m2 = tg;
     fy2 = fy1; fy1 = fy;
     th_m4 = th_m3; th_m3 = th;
   }
