@@ -49,6 +49,7 @@ struct swe_sim {
   int nx, ny, W, H, N;
   double dx, dy, eps4, R, dlam, dphi, totalArea;
   std::vector<double> geom[SWE_GEOM_NROWS];
+  std::vector<double> recip[3];
   cudaStream_t st = nullptr;
   double* d_b = nullptr;
   double* d_A[3] = {nullptr, nullptr, nullptr};
@@ -179,6 +180,8 @@ swe::Metric metric(const swe_sim* s) {
   m.dyRowS = g + SWE_GEOM_DYROWS * H; m.dyCFL = g + SWE_GEOM_DYCFL * H;
   m.bedPhi = g + SWE_GEOM_BEDPHI * H; m.geoCoef = g + SWE_GEOM_GEOCOEF * H;
   m.fRow = g + SWE_GEOM_FROW * H; m.tanPhi = g + SWE_GEOM_TANPHI * H;
+  m.rdxRow = g + (SWE_GEOM_NROWS + 0) * H; m.rdyRowN = g + (SWE_GEOM_NROWS + 1) * H;
+  m.rdyRowS = g + (SWE_GEOM_NROWS + 2) * H;
   m.R = s->R;
   return m;
 }
@@ -230,7 +233,10 @@ int launch_bc(swe_sim* s, double* const* f, int respect_stop) {
 int enqueue_step(swe_sim* s, int mode, double dt, double t_end) {
   swe::k_prepare<<<1, 32, 0, s->st>>>(s->d_ctl, prep_args(s, mode, dt, t_end));
   CU(cudaGetLastError());
-  int rc = launch_bc(s, s->d_A, 0);
+  // Host-checked dt (mode 0) never reaches here refused.  In the device loop
+  // a refused step (t reached t_end) changes nothing, ghosts included, as the
+  // drivers' `while (sim.t < T)` loop stops calling step().
+  int rc = launch_bc(s, s->d_A, mode == 0 ? 0 : 1);
   if (rc) return rc;
   swe::StageArgs a1 = stage_args(s, s->d_A, s->d_B);
   swe::k_stage<1><<<s->grid, swe::BX, 0, s->st>>>(a1, s->d_ctl);
@@ -288,10 +294,23 @@ double* field_ptr(swe_sim* s, int f) {
   }
 }
 
+// Reciprocals of the three flux divisors (rows after the 13 metric rows).
+void fill_reciprocals(swe_sim* s) {
+  const int src[3] = {SWE_GEOM_DXROW, SWE_GEOM_DYROWN, SWE_GEOM_DYROWS};
+  for (int q = 0; q < 3; q++) {
+    s->recip[q].resize(s->H);
+    for (int j = 0; j < s->H; j++) s->recip[q][j] = 1.0 / s->geom[src[q]][j];
+  }
+}
+
 int upload_geom(swe_sim* s) {
+  fill_reciprocals(s);
   for (int r = 0; r < SWE_GEOM_NROWS; r++)
     CU(cudaMemcpyAsync(s->d_geom + (size_t)r * s->H, s->geom[r].data(), sizeof(double) * s->H,
                        cudaMemcpyHostToDevice, s->st));
+  for (int q = 0; q < 3; q++)
+    CU(cudaMemcpyAsync(s->d_geom + (size_t)(SWE_GEOM_NROWS + q) * s->H, s->recip[q].data(),
+                       sizeof(double) * s->H, cudaMemcpyHostToDevice, s->st));
   return SWE_OK;
 }
 
@@ -376,7 +395,7 @@ int swe_create(const swe_options* o, const double* b, const double* h, swe_sim**
   CUB(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
   CUB(cudaMalloc(&s->d_b, nb));
   for (int q = 0; q < 3; q++) { CUB(cudaMalloc(&s->d_A[q], nb)); CUB(cudaMalloc(&s->d_B[q], nb)); }
-  CUB(cudaMalloc(&s->d_geom, sizeof(double) * SWE_GEOM_NROWS * s->H));
+  CUB(cudaMalloc(&s->d_geom, sizeof(double) * (SWE_GEOM_NROWS + 3) * s->H));
   CUB(cudaMalloc(&s->d_part, sizeof(double) * 3 * s->part_cap));
   CUB(cudaMalloc(&s->d_rows, sizeof(double) * std::max(1, s->ny)));
   CUB(cudaMalloc(&s->d_ctl, sizeof(swe::Control)));
@@ -447,8 +466,8 @@ int swe_set_geom(swe_sim* s, int row, const double* in) {
   if (!s || !in) return fail(SWE_EINVAL, "null argument");
   if (row < 0 || row >= SWE_GEOM_NROWS) return fail(SWE_EINVAL, "unknown metric row id");
   std::memcpy(s->geom[row].data(), in, sizeof(double) * s->H);
-  CU(cudaMemcpyAsync(s->d_geom + (size_t)row * s->H, s->geom[row].data(), sizeof(double) * s->H,
-                     cudaMemcpyHostToDevice, s->st));
+  const int rc = upload_geom(s);
+  if (rc) return rc;
   CU(cudaStreamSynchronize(s->st));
   s->cfl_valid = false;
   return SWE_OK;

@@ -65,8 +65,18 @@ struct Control {
 struct Metric {   // per-row divisors (src/geometry.mjs)
   const double* dxRow; const double* dyRowN; const double* dyRowS; const double* dyCFL;
   const double* bedPhi; const double* geoCoef; const double* fRow; const double* tanPhi;
+  // 1/dxRow, 1/dyRowN, 1/dyRowS, formed on the host with the same IEEE
+  // division, so theta/dxRow == rdxRow exactly when theta == 1
+  const double* rdxRow; const double* rdyRowN; const double* rdyRowS;
   double R;
 };
+
+// x / d, skipping the division when the factor z of x is +-0: then x is
+// +-0 or NaN, and +-0 / d == +-0, NaN / d == NaN for the finite or
+// infinite positive divisors of the metric.
+__device__ __forceinline__ double div_unless_zero(double x, double z, double d) {
+  return z == 0 ? x : x / d;
+}
 
 struct StageArgs {
   int W, H, nx, ny;
@@ -240,7 +250,10 @@ __global__ void k_apply_bc(BCArgs a, const Control* ctl, int respect_stop) {
 // theta for every cell, src/swe.mjs:308-629); MODE 1: stage 1
 // (src/swe.mjs:790-796); MODE 2: stage 2 + epilogue (src/swe.mjs:798-813).
 template <int MODE>
-__global__ void __launch_bounds__(BX, 3) k_stage(StageArgs a, Control* ctl) {
+#ifndef SWE_STAGE_MIN_BLOCKS
+#define SWE_STAGE_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a, Control* ctl) {
   if (MODE != 0 && ctl->stop) return;
   __shared__ double s_b[3][BX], s_h[3][BX], s_U[3][BX], s_V[3][BX];   // state ring
   __shared__ double s_xs[2][4][BX];                                  // x slopes ring (sE,sB,sU,sV)
@@ -282,9 +295,14 @@ __global__ void __launch_bounds__(BX, 3) k_stage(StageArgs a, Control* ctl) {
       const int k = r * W + gi;
       b_c = __ldg(a.b + k); h_c = __ldg(a.h + k);
       const double hu_c = __ldg(a.hu + k), hv_c = __ldg(a.hv + k);
-      const double den = vel_den(h_c, eps4);
-      U_c = vel_num(hu_c, h_c) / den;
-      V_c = vel_num(hv_c, h_c) / den;
+      if (h_c == 0) {                 // +-0 / den == +-0 and NaN / den == NaN: no division needed
+        U_c = vel_num(hu_c, h_c);
+        V_c = vel_num(hv_c, h_c);
+      } else {
+        const double den = vel_den(h_c, eps4);
+        U_c = vel_num(hu_c, h_c) / den;
+        V_c = vel_num(hv_c, h_c) / den;
+      }
     }
     const int sr = (r + 3) % 3;     // slot of row r (r >= -3, so every slot index here is >= 0)
     s_b[sr][c] = b_c; s_h[sr][c] = h_c; s_U[sr][c] = U_c; s_V[sr][c] = V_c;
@@ -327,12 +345,12 @@ __global__ void __launch_bounds__(BX, 3) k_stage(StageArgs a, Control* ctl) {
       {
         const double hP = jmax0(eC + 0.5 * xsE - (bk + 0.5 * xsB));
         const double hM = jmax0(eC - 0.5 * xsE - (bk - 0.5 * xsB));
-        tb0 = -SWE_G * 0.5 * (hP + hM) * xsB / a.m.dxRow[j1];
+        tb0 = div_unless_zero(-SWE_G * 0.5 * (hP + hM) * xsB, xsB, a.m.dxRow[j1]);
       }
       {
         const double hP = jmax0(eC + 0.5 * nsE - (bk + 0.5 * nsB));
         const double hM = jmax0(eC - 0.5 * nsE - (bk - 0.5 * nsB));
-        tb1 = -SWE_G * 0.5 * (hP + hM) * nsB / a.m.bedPhi[j1];
+        tb1 = div_unless_zero(-SWE_G * 0.5 * (hP + hM) * nsB, nsB, a.m.bedPhi[j1]);
         if (sph) tg = a.m.geoCoef[j1] * SWE_G * (hP * hP + hM * hM);
       }
     }
@@ -363,13 +381,21 @@ __global__ void __launch_bounds__(BX, 3) k_stage(StageArgs a, Control* ctl) {
       const int f2 = (r + 4) % 3;   // slot of row r-2
       const double fxE = s_fx[f2][0][c], fxW = s_fx[f2][0][c - 1];
       const double fyN = fy.M, fyS = fy1.M;
-      double out = 0;
-      if (fxE > 0) out += fxE / a.m.dxRow[j2];
-      if (fxW < 0) out -= fxW / a.m.dxRow[j2];
-      if (fyN > 0) out += fyN / a.m.dyRowN[j2];
-      if (fyS < 0) out -= fyS / a.m.dyRowS[j2];
       const double avail = h_m2;
-      if (out * dt > avail) th = avail > 0 ? avail / (out * dt) : 0;
+      // The reference's out-budget is a sum of non-negative quotients.  The
+      // same sum with reciprocal multiplies is within 1e-15 relative of it,
+      // so when that estimate sits clearly below the water available the
+      // limiter cannot fire and theta is 1 without forming the quotients.
+      const double est = ((fxE > 0 ? fxE : 0) - (fxW < 0 ? fxW : 0)) * a.m.rdxRow[j2]
+                       + (fyN > 0 ? fyN : 0) * a.m.rdyRowN[j2] - (fyS < 0 ? fyS : 0) * a.m.rdyRowS[j2];
+      if (!(est * dt * (1 + 1e-12) < avail)) {
+        double out = 0;
+        if (fxE > 0) out += fxE / a.m.dxRow[j2];
+        if (fxW < 0) out -= fxW / a.m.dxRow[j2];
+        if (fyN > 0) out += fyN / a.m.dyRowN[j2];
+        if (fyS < 0) out -= fyS / a.m.dyRowS[j2];
+        if (out * dt > avail) th = avail > 0 ? avail / (out * dt) : 0;
+      }
     }
     s_th[(r + 4) & 1][c] = th;      // slot of row r-2
 
@@ -385,14 +411,14 @@ __global__ void __launch_bounds__(BX, 3) k_stage(StageArgs a, Control* ctl) {
         if (gi - 1 >= 1 && gi - 1 < W - 2) {
           const double M = s_fx[f3][0][c - 1];
           const double thf = M >= 0 ? s_th[ts][c - 1] : th_m3;
-          const double inv = thf / a.m.dxRow[j3];
+          const double inv = thf == 1 ? a.m.rdxRow[j3] : thf / a.m.dxRow[j3];
           ah += M * inv; ahu += (s_fx[f3][1][c - 1] + s_fx[f3][4][c - 1]) * inv; ahv += s_fx[f3][2][c - 1] * inv;
         }
         // east face (c|c+1), cell is its left side
         if (gi >= 1 && gi < W - 2) {
           const double M = s_fx[f3][0][c];
           const double thf = M >= 0 ? th_m3 : s_th[ts][c + 1];
-          const double inv = thf / a.m.dxRow[j3];
+          const double inv = thf == 1 ? a.m.rdxRow[j3] : thf / a.m.dxRow[j3];
           ah -= M * inv; ahu -= (s_fx[f3][1][c] + s_fx[f3][3][c]) * inv; ahv -= s_fx[f3][2][c] * inv;
         }
       }
@@ -400,13 +426,13 @@ __global__ void __launch_bounds__(BX, 3) k_stage(StageArgs a, Control* ctl) {
         // south face (r-4|r-3), cell is its upper side
         if (j3 - 1 >= 1 && j3 - 1 < H - 2) {
           const double thf = fy2.M >= 0 ? th_m4 : th_m3;
-          const double invR = thf / a.m.dyRowS[j3];
+          const double invR = thf == 1 ? a.m.rdyRowS[j3] : thf / a.m.dyRowS[j3];
           ah += fy2.M * invR; ahv += (fy2.N + fy2.pR) * invR; ahu += fy2.T * invR;
         }
         // north face (r-3|r-2), cell is its lower side
         if (j3 >= 1 && j3 < H - 2) {
           const double thf = fy1.M >= 0 ? th_m3 : th;
-          const double invL = thf / a.m.dyRowN[j3];
+          const double invL = thf == 1 ? a.m.rdyRowN[j3] : thf / a.m.dyRowN[j3];
           ah -= fy1.M * invL; ahv -= (fy1.N + fy1.pL) * invL; ahu -= fy1.T * invL;
         }
       }
