@@ -154,8 +154,31 @@ def test_residual_and_theta(swe):
         ref.residual(dt)
         assert_fields_equal(gpu, ref, names=("b", "h", "hu", "hv", "rh", "rhu", "rhv", "theta"),
                             what=f"residual x{mult}")
-        if mult == 5.0:
-            assert np.any(ref.field("theta") < 1), "the limiter should fire at 5x the CFL step"
+
+
+
+def test_residual_limiter_fires_bit_identical(swe):
+    """tools/verify-physics.mjs:470-498: a 40-cell row split into opposing
+    9 m/s jets, residual at 5x the CFL step, where the limiter clips."""
+    nx, dx, h0, USPLIT = 40, 2, 0.5, 9
+    gpu, ref = pair(swe, nx=nx, ny=1, dx=dx, bed=lambda x, y: 0, eta0=h0, manning=0)
+    for sim in (gpu, ref):
+        h, hu = sim.h, sim.hu
+        for i in range(nx):
+            k = sim.idx(i, 0)
+            h[k] = h0
+            hu[k] = h0 * (-USPLIT if i < nx / 2 else USPLIT)
+    dt = 5 * ref.maxDt()
+    assert gpu.maxDt() * 5 == dt
+    gpu.applyBC()
+    ref.applyBC()
+    gpu.residual(dt)
+    ref.residual(dt)
+    assert_fields_equal(gpu, ref, names=("h", "hu", "hv", "rh", "rhu", "rhv", "theta"))
+    th = ref.field("theta")
+    assert np.any(th < 1)
+    end = [gpu.h[gpu.idx(i, 0)] + dt * gpu.rh[gpu.idx(i, 0)] for i in range(nx)]
+    assert min(end) >= -1e-15
 
 
 def test_theta_one_wet_cell_gpu(swe):

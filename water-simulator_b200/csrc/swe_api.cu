@@ -239,13 +239,13 @@ int enqueue_step(swe_sim* s, int mode, double dt, double t_end) {
   int rc = launch_bc(s, s->d_A, mode == 0 ? 0 : 1);
   if (rc) return rc;
   swe::StageArgs a1 = stage_args(s, s->d_A, s->d_B);
-  swe::k_stage<1><<<s->grid, swe::BX, 0, s->st>>>(a1, s->d_ctl);
+  swe::k_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a1, s->d_ctl);
   CU(cudaGetLastError());
   rc = launch_bc(s, s->d_B, 1);
   if (rc) return rc;
   swe::StageArgs a2 = stage_args(s, s->d_B, s->d_A);
   if (s->keep_h0) { a2.h0c = s->d_h0[0]; a2.hu0c = s->d_h0[1]; a2.hv0c = s->d_h0[2]; }
-  swe::k_stage<2><<<s->grid, swe::BX, 0, s->st>>>(a2, s->d_ctl);
+  swe::k_stage<2><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a2, s->d_ctl);
   CU(cudaGetLastError());
   return SWE_OK;
 }
@@ -326,7 +326,7 @@ void free_all(swe_sim* s) {
 
 int choose_rows_per_cta(const swe_sim* s) {
   const char* env = std::getenv("SWE_B200_ROWS_PER_CTA");
-  if (env) { const int v = std::atoi(env); if (v >= 4) return v; }
+  if (env) { const int v = std::atoi(env); if (v >= 4) return std::min(v, swe::RY_MAX); }
   return 32;
 }
 
@@ -392,6 +392,9 @@ int swe_create(const swe_options* o, const double* b, const double* h, swe_sim**
     cudaError_t e_ = (call);                                                               \
     if (e_ != cudaSuccess) return bail(fail(SWE_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_))); \
   } while (0)
+  CUB(cudaFuncSetAttribute(swe::k_stage<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, swe::STAGE_SMEM_BYTES));
+  CUB(cudaFuncSetAttribute(swe::k_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, swe::STAGE_SMEM_BYTES));
+  CUB(cudaFuncSetAttribute(swe::k_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, swe::STAGE_SMEM_BYTES));
   CUB(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
   CUB(cudaMalloc(&s->d_b, nb));
   for (int q = 0; q < 3; q++) { CUB(cudaMalloc(&s->d_A[q], nb)); CUB(cudaMalloc(&s->d_B[q], nb)); }
@@ -629,7 +632,7 @@ int swe_residual(swe_sim* s, double dt) {
   CU(cudaGetLastError());
   swe::StageArgs a = stage_args(s, s->d_A, nullptr);
   a.rh = s->d_res[0]; a.rhu = s->d_res[1]; a.rhv = s->d_res[2]; a.theta = s->d_res[3];
-  swe::k_stage<0><<<s->grid, swe::BX, 0, s->st>>>(a, s->d_ctl);
+  swe::k_stage<0><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a, s->d_ctl);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(s->st));
   return SWE_OK;
@@ -845,14 +848,14 @@ int swe_step_timed(swe_sim* s, double dt, double* ms) {
   rc = launch_bc(s, s->d_A, 0);
   if (rc) return rc;
   CU(cudaEventRecord(ev[2], s->st));
-  swe::k_stage<1><<<s->grid, swe::BX, 0, s->st>>>(stage_args(s, s->d_A, s->d_B), s->d_ctl);
+  swe::k_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(stage_args(s, s->d_A, s->d_B), s->d_ctl);
   CU(cudaEventRecord(ev[3], s->st));
   rc = launch_bc(s, s->d_B, 1);
   if (rc) return rc;
   CU(cudaEventRecord(ev[4], s->st));
   swe::StageArgs a2 = stage_args(s, s->d_B, s->d_A);
   if (s->keep_h0) { a2.h0c = s->d_h0[0]; a2.hu0c = s->d_h0[1]; a2.hv0c = s->d_h0[2]; }
-  swe::k_stage<2><<<s->grid, swe::BX, 0, s->st>>>(a2, s->d_ctl);
+  swe::k_stage<2><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a2, s->d_ctl);
   CU(cudaEventRecord(ev[5], s->st));
   CU(cudaEventSynchronize(ev[5]));
   for (int q = 0; q < 5; q++) {

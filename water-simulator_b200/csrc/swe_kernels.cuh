@@ -249,25 +249,42 @@ __global__ void k_apply_bc(BCArgs a, const Control* ctl, int respect_stop) {
 // Fused residual + stage update.  MODE 0: residual only (rh, rhu, rhv,
 // theta for every cell, src/swe.mjs:308-629); MODE 1: stage 1
 // (src/swe.mjs:790-796); MODE 2: stage 2 + epilogue (src/swe.mjs:798-813).
-template <int MODE>
+constexpr int RY_MAX = 64;                  // output rows per CTA, at most
+constexpr int MROWS = RY_MAX + 6;           // metric rows a CTA touches
+enum { M_DX, M_RDX, M_DYN, M_RDYN, M_DYS, M_RDYS, M_BED, M_GEO, M_F, M_TAN, M_CFL, M_COUNT };
+// dynamic shared memory of k_stage: state ring 4x6 rows, x slopes 2x4,
+// x faces 3x5, theta 2 (all BX wide), then the metric rows
+constexpr int STAGE_SMEM_BYTES = (49 * BX + M_COUNT * MROWS) * 8;
+
 #ifndef SWE_STAGE_MIN_BLOCKS
 #define SWE_STAGE_MIN_BLOCKS 3
 #endif
+template <int MODE>
 __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a, Control* ctl) {
   if (MODE != 0 && ctl->stop) return;
-  __shared__ double s_b[3][BX], s_h[3][BX], s_U[3][BX], s_V[3][BX];   // state ring
-  __shared__ double s_xs[2][4][BX];                                  // x slopes ring (sE,sB,sU,sV)
-  __shared__ double s_fx[3][5][BX];                                  // x faces ring (M,N,T,pL,pR)
-  __shared__ double s_th[2][BX];                                     // theta ring
+  // state ring, 4 rows deep: b, h, U, V are read by neighbours (rows r-1),
+  // h, hu, hv, U of row r-3 by the cell's own thread in S5
+  extern __shared__ double smem[];                                   // STAGE_SMEM_BYTES
+  double (*s_b)[BX] = reinterpret_cast<double (*)[BX]>(smem);
+  double (*s_h)[BX] = s_b + 4;
+  double (*s_U)[BX] = s_b + 8;
+  double (*s_V)[BX] = s_b + 12;
+  double (*s_hu)[BX] = s_b + 16;
+  double (*s_hv)[BX] = s_b + 20;
+  double (*s_xs)[4][BX] = reinterpret_cast<double (*)[4][BX]>(smem + 24 * BX);   // x slopes ring (sE,sB,sU,sV)
+  double (*s_fx)[5][BX] = reinterpret_cast<double (*)[5][BX]>(smem + 32 * BX);   // x faces ring (M,N,T,pL,pR)
+  double (*s_th)[BX] = reinterpret_cast<double (*)[BX]>(smem + 47 * BX);         // theta ring
+  double (*s_m)[MROWS] = reinterpret_cast<double (*)[MROWS]>(smem + 49 * BX);    // the CTA's metric rows
   __shared__ double s_red[2][BX / 32];
 
   const int c = threadIdx.x;
   const int W = a.W, H = a.H;
   const int gi = (int)blockIdx.x * SX - HALO + c;
   const bool colIn = gi >= 0 && gi < W;
-  const int RY = (H + gridDim.y - 1) / gridDim.y;
+  const int RY = (H + gridDim.y - 1) / gridDim.y;     // <= RY_MAX (host)
   const int y0 = (int)blockIdx.y * RY;
   const int y1 = min(y0 + RY, H);            // output rows [y0, y1)
+  const int mbase = y0 - 3;                  // metric row m = j - mbase
   const double dt = ctl->dt;
   const double dry = a.minDepth, eps4 = a.eps4;
   const bool order2 = a.order >= 2;
@@ -277,10 +294,24 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
   const bool outCol = c >= HALO && c < HALO + SX && colIn;
   const bool interiorCol = gi >= 2 && gi < W - 2;
 
+  // metric rows of this chunk into shared memory (broadcast reads later)
+  for (int q = c; q < M_COUNT * MROWS; q += BX) {
+    const int f = q / MROWS, m = q % MROWS, j = m + mbase;
+    double v = 0;
+    if (j >= 0 && j < H && m < RY + 6) {
+      const double* src = f == M_DX ? a.m.dxRow : f == M_RDX ? a.m.rdxRow : f == M_DYN ? a.m.dyRowN :
+                          f == M_RDYN ? a.m.rdyRowN : f == M_DYS ? a.m.dyRowS : f == M_RDYS ? a.m.rdyRowS :
+                          f == M_BED ? a.m.bedPhi : f == M_GEO ? a.m.geoCoef : f == M_F ? a.m.fRow :
+                          f == M_TAN ? a.m.tanPhi : a.m.dyCFL;
+      v = src[j];
+    }
+    s_m[f][m] = v;
+  }
+  __syncthreads();
+
   // carried registers (same column)
   double b_m1 = 0, h_m1 = 0, U_m1 = 0, V_m1 = 0;     // row r-1
   double b_m2 = 0, h_m2 = 0, U_m2 = 0, V_m2 = 0;     // row r-2
-  double U_m3 = 0;                                   // row r-3
   double ysE = 0, ysB = 0, ysU = 0, ysV = 0;         // y slopes of row r-2
   double tb0_m2 = 0, tb1_m2 = 0, tg_m2 = 0;          // bed terms of row r-2 (computed last row)
   double tb0_m3 = 0, tb1_m3 = 0, tg_m3 = 0;          // bed terms of row r-3
@@ -288,28 +319,52 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
   double th_m3 = 1, th_m4 = 1;
   double locMax = 0, locFl = 0;
 
-  for (int r = y0 - 3; r <= y1 + 2; ++r) {
-    // ---- S1: row r ------------------------------------------------------
-    double b_c = 0, h_c = 0, U_c = 0, V_c = 0;
+  // prefetch of the next row of the input state, and (stage 2) of U0 one
+  // row ahead of its use in S5
+  double pb = 0, ph = 0, phu = 0, phv = 0;
+  double p0h = 0, p0hu = 0, p0hv = 0;
+  {
+    const int r = y0 - 3;
     if (colIn && r >= 0 && r < H) {
       const int k = r * W + gi;
-      b_c = __ldg(a.b + k); h_c = __ldg(a.h + k);
-      const double hu_c = __ldg(a.hu + k), hv_c = __ldg(a.hv + k);
-      if (h_c == 0) {                 // +-0 / den == +-0 and NaN / den == NaN: no division needed
-        U_c = vel_num(hu_c, h_c);
-        V_c = vel_num(hv_c, h_c);
-      } else {
-        const double den = vel_den(h_c, eps4);
-        U_c = vel_num(hu_c, h_c) / den;
-        V_c = vel_num(hv_c, h_c) / den;
+      pb = __ldg(a.b + k); ph = __ldg(a.h + k); phu = __ldg(a.hu + k); phv = __ldg(a.hv + k);
+    }
+  }
+
+  for (int r = y0 - 3; r <= y1 + 2; ++r) {
+    // ---- S1: row r (prefetched), issue the loads of row r+1 -------------
+    const double b_c = pb, h_c = ph, hu_c = phu, hv_c = phv;
+    if (colIn && r + 1 >= 0 && r + 1 < H && r + 1 <= y1 + 2) {
+      const int k = (r + 1) * W + gi;
+      pb = __ldg(a.b + k); ph = __ldg(a.h + k); phu = __ldg(a.hu + k); phv = __ldg(a.hv + k);
+    } else {
+      pb = 0; ph = 0; phu = 0; phv = 0;
+    }
+    double U0h = 0, U0hu = 0, U0hv = 0;              // U0 of row r-3 (stage 2)
+    if (MODE == 2) {
+      U0h = p0h; U0hu = p0hu; U0hv = p0hv;
+      const int jn = r - 2;
+      if (outCol && jn >= y0 && jn < y1) {
+        const int k = jn * W + gi;
+        p0h = a.oh[k]; p0hu = a.ohu[k]; p0hv = a.ohv[k];
       }
     }
-    const int sr = (r + 3) % 3;     // slot of row r (r >= -3, so every slot index here is >= 0)
+    double U_c = 0, V_c = 0;
+    if (h_c == 0) {                 // +-0 / den == +-0 and NaN / den == NaN: no division needed
+      U_c = vel_num(hu_c, h_c);
+      V_c = vel_num(hv_c, h_c);
+    } else {
+      const double den = vel_den(h_c, eps4);
+      U_c = vel_num(hu_c, h_c) / den;
+      V_c = vel_num(hv_c, h_c) / den;
+    }
+    const int sr = (r + 4) & 3;     // ring slot of row r (r >= -3)
     s_b[sr][c] = b_c; s_h[sr][c] = h_c; s_U[sr][c] = U_c; s_V[sr][c] = V_c;
+    s_hu[sr][c] = hu_c; s_hv[sr][c] = hv_c;
 
     // ---- S2: slopes and bed term of row r-1 --------------------------------
     const int j1 = r - 1;
-    const int sr1 = (r + 5) % 3;    // slot of row r-1
+    const int sr1 = (r + 3) & 3;    // slot of row r-1
     double xsE = 0, xsB = 0, xsU = 0, xsV = 0;
     double nsE = 0, nsB = 0, nsU = 0, nsV = 0;         // y slopes of row r-1
     if (order2 && j1 >= 1 && j1 < H - 1 && gi >= 1 && gi < W - 1 && c >= 1 && c < BX - 1) {
@@ -341,17 +396,18 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
     double tb0 = 0, tb1 = 0, tg = 0;
     if (bedOn && j1 >= 2 && j1 < H - 2 && interiorCol) {
       // src/swe.mjs:570-598
+      const int m1 = j1 - mbase;
       const double bk = b_m1, eC = bk + h_m1;
       {
         const double hP = jmax0(eC + 0.5 * xsE - (bk + 0.5 * xsB));
         const double hM = jmax0(eC - 0.5 * xsE - (bk - 0.5 * xsB));
-        tb0 = div_unless_zero(-SWE_G * 0.5 * (hP + hM) * xsB, xsB, a.m.dxRow[j1]);
+        tb0 = div_unless_zero(-SWE_G * 0.5 * (hP + hM) * xsB, xsB, s_m[M_DX][m1]);
       }
       {
         const double hP = jmax0(eC + 0.5 * nsE - (bk + 0.5 * nsB));
         const double hM = jmax0(eC - 0.5 * nsE - (bk - 0.5 * nsB));
-        tb1 = div_unless_zero(-SWE_G * 0.5 * (hP + hM) * nsB, nsB, a.m.bedPhi[j1]);
-        if (sph) tg = a.m.geoCoef[j1] * SWE_G * (hP * hP + hM * hM);
+        tb1 = div_unless_zero(-SWE_G * 0.5 * (hP + hM) * nsB, nsB, s_m[M_BED][m1]);
+        if (sph) tg = s_m[M_GEO][m1] * SWE_G * (hP * hP + hM * hM);
       }
     }
     __syncthreads();
@@ -377,8 +433,10 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
 
     // ---- S4: theta of row r-2 (src/swe.mjs:511-529) -------------------------
     double th = 1;
-    if (dt > 0 && j2 >= 1 && j2 < H - 1 && gi >= 1 && gi < W - 1 && c >= 1 && c < BX - 1) {
+    if (dt > 0 && j2 >= 1 && j2 < H - 1 && gi >= 1 && gi < W - 1 && c >= 1 && c < BX - 1 &&
+        j2 >= y0 - 1 && j2 <= y1) {
       const int f2 = (r + 4) % 3;   // slot of row r-2
+      const int m2 = j2 - mbase;
       const double fxE = s_fx[f2][0][c], fxW = s_fx[f2][0][c - 1];
       const double fyN = fy.M, fyS = fy1.M;
       const double avail = h_m2;
@@ -386,14 +444,14 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
       // same sum with reciprocal multiplies is within 1e-15 relative of it,
       // so when that estimate sits clearly below the water available the
       // limiter cannot fire and theta is 1 without forming the quotients.
-      const double est = ((fxE > 0 ? fxE : 0) - (fxW < 0 ? fxW : 0)) * a.m.rdxRow[j2]
-                       + (fyN > 0 ? fyN : 0) * a.m.rdyRowN[j2] - (fyS < 0 ? fyS : 0) * a.m.rdyRowS[j2];
+      const double est = ((fxE > 0 ? fxE : 0) - (fxW < 0 ? fxW : 0)) * s_m[M_RDX][m2]
+                       + (fyN > 0 ? fyN : 0) * s_m[M_RDYN][m2] - (fyS < 0 ? fyS : 0) * s_m[M_RDYS][m2];
       if (!(est * dt * (1 + 1e-12) < avail)) {
         double out = 0;
-        if (fxE > 0) out += fxE / a.m.dxRow[j2];
-        if (fxW < 0) out -= fxW / a.m.dxRow[j2];
-        if (fyN > 0) out += fyN / a.m.dyRowN[j2];
-        if (fyS < 0) out -= fyS / a.m.dyRowS[j2];
+        if (fxE > 0) out += fxE / s_m[M_DX][m2];
+        if (fxW < 0) out -= fxW / s_m[M_DX][m2];
+        if (fyN > 0) out += fyN / s_m[M_DYN][m2];
+        if (fyS < 0) out -= fyS / s_m[M_DYS][m2];
         if (out * dt > avail) th = avail > 0 ? avail / (out * dt) : 0;
       }
     }
@@ -403,22 +461,24 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
     const int j3 = r - 3;
     if (outCol && j3 >= y0 && j3 < y1) {
       const int k = j3 * W + gi;
+      const int m3 = j3 - mbase;
       const int f3 = (r + 3) % 3;   // slot of row r-3
       const int ts = (r + 5) & 1;   // theta slot of row r-3
+      const int s3 = (r + 1) & 3;   // state ring slot of row r-3
       double ah = 0, ahu = 0, ahv = 0;
       if (j3 >= 2 && j3 < H - 2) {
         // west face (c-1|c), cell is its right side
         if (gi - 1 >= 1 && gi - 1 < W - 2) {
           const double M = s_fx[f3][0][c - 1];
           const double thf = M >= 0 ? s_th[ts][c - 1] : th_m3;
-          const double inv = thf == 1 ? a.m.rdxRow[j3] : thf / a.m.dxRow[j3];
+          const double inv = thf == 1 ? s_m[M_RDX][m3] : thf / s_m[M_DX][m3];
           ah += M * inv; ahu += (s_fx[f3][1][c - 1] + s_fx[f3][4][c - 1]) * inv; ahv += s_fx[f3][2][c - 1] * inv;
         }
         // east face (c|c+1), cell is its left side
         if (gi >= 1 && gi < W - 2) {
           const double M = s_fx[f3][0][c];
           const double thf = M >= 0 ? th_m3 : s_th[ts][c + 1];
-          const double inv = thf == 1 ? a.m.rdxRow[j3] : thf / a.m.dxRow[j3];
+          const double inv = thf == 1 ? s_m[M_RDX][m3] : thf / s_m[M_DX][m3];
           ah -= M * inv; ahu -= (s_fx[f3][1][c] + s_fx[f3][3][c]) * inv; ahv -= s_fx[f3][2][c] * inv;
         }
       }
@@ -426,18 +486,18 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
         // south face (r-4|r-3), cell is its upper side
         if (j3 - 1 >= 1 && j3 - 1 < H - 2) {
           const double thf = fy2.M >= 0 ? th_m4 : th_m3;
-          const double invR = thf == 1 ? a.m.rdyRowS[j3] : thf / a.m.dyRowS[j3];
+          const double invR = thf == 1 ? s_m[M_RDYS][m3] : thf / s_m[M_DYS][m3];
           ah += fy2.M * invR; ahv += (fy2.N + fy2.pR) * invR; ahu += fy2.T * invR;
         }
         // north face (r-3|r-2), cell is its lower side
         if (j3 >= 1 && j3 < H - 2) {
           const double thf = fy1.M >= 0 ? th_m3 : th;
-          const double invL = thf == 1 ? a.m.rdyRowN[j3] : thf / a.m.dyRowN[j3];
+          const double invL = thf == 1 ? s_m[M_RDYN][m3] : thf / s_m[M_DYN][m3];
           ah -= fy1.M * invL; ahv -= (fy1.N + fy1.pL) * invL; ahu -= fy1.T * invL;
         }
       }
       const bool interior = interiorCol && j3 >= 2 && j3 < H - 2;
-      const double hin = __ldg(a.h + k), huin = __ldg(a.hu + k), hvin = __ldg(a.hv + k);
+      const double hin = s_h[s3][c], huin = s_hu[s3][c], hvin = s_hv[s3][c];
       if (interior) {
         if (bedOn) {
           ahu += tb0_m3;
@@ -445,7 +505,7 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
           if (sph) ahv += tg_m3;
         }
         if (sph) {
-          const double fe = a.m.fRow[j3] + U_m3 * (a.m.tanPhi[j3] / a.m.R);
+          const double fe = s_m[M_F][m3] + s_U[s3][c] * (s_m[M_TAN][m3] / a.m.R);
           ahu += fe * hvin;
           ahv -= fe * huin;
         } else if (corOn) {
@@ -463,7 +523,7 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
         }
         a.oh[k] = nh; a.ohu[k] = nhu; a.ohv[k] = nhv;
       } else {
-        const double h0 = a.oh[k], hu0 = a.ohu[k], hv0 = a.ohv[k];   // U0 (in place)
+        const double h0 = U0h, hu0 = U0hu, hv0 = U0hv;   // U0 (in place)
         if (a.h0c) { a.h0c[k] = h0; a.hu0c[k] = hu0; a.hv0c[k] = hv0; }
         double nh = 0.5 * (h0 + hin + dt * ah);
         double nhu = 0.5 * (hu0 + huin + dt * ahu);
@@ -506,8 +566,8 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
             const double cc = sqrt(SWE_G * nh);
             const double den = vel_den(nh, eps4);
             const double u = fabs(vel_num(nhu, nh) / den), v = fabs(vel_num(nhv, nh) / den);
-            const double s = (u + cc) / a.m.dxRow[j3] + (v + cc) / a.m.dyCFL[j3];
-            if (s > locMax) locMax = s;
+            const double sr5 = (u + cc) / s_m[M_DX][m3] + (v + cc) / s_m[M_CFL][m3];
+            if (sr5 > locMax) locMax = sr5;
           }
         }
         a.oh[k] = nh; a.ohu[k] = nhu; a.ohv[k] = nhv;
@@ -515,7 +575,6 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
     }
 
     // ---- rotate ------------------------------------------------------------
-    U_m3 = U_m2;
     b_m2 = b_m1; h_m2 = h_m1; U_m2 = U_m1; V_m2 = V_m1;
     b_m1 = b_c; h_m1 = h_c; U_m1 = U_c; V_m1 = V_c;
     ysE = nsE; ysB = nsB; ysU = nsU; ysV = nsV;
