@@ -413,34 +413,23 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
     __syncthreads();
 
     // ---- S3: x face (c|c+1) of row r-1, y face (r-2|r-1) --------------------
-    // Both faces of this row step are solved together, branch-free, so their
-    // dependency chains interleave; a warp whose faces are all dry skips it.
-    const int j2 = r - 2;
-    const bool xOn = j1 >= 2 && j1 < H - 2 && gi >= 1 && gi < W - 2 && c < BX - 1 && j1 >= y0 - 1 && j1 <= y1;
-    const bool yOn = j2 >= 1 && j2 < H - 2 && gi >= 2 && gi < W - 2 && j2 >= y0 - 2 && j2 <= y1;
-    Face fx = {0, 0, 0, 0, 0}, fy = {0, 0, 0, 0, 0};
-    {
-      const int cn = c < BX - 1 ? c + 1 : c;
-      const FaceState qx = face_state(b_m1, h_m1, U_m1, V_m1, xsE, xsB, xsU, xsV,
-                                      s_b[sr1][cn], s_h[sr1][cn], s_U[sr1][cn], s_V[sr1][cn],
-                                      s_xs[xsr][0][cn], s_xs[xsr][1][cn], s_xs[xsr][2][cn], s_xs[xsr][3][cn]);
-      // lower cell row r-2 (slopes ys*), upper cell row r-1 (slopes ns*); v is normal
-      const FaceState qy = face_state(b_m2, h_m2, V_m2, U_m2, ysE, ysB, ysV, ysU,
-                                      b_m1, h_m1, V_m1, U_m1, nsE, nsB, nsV, nsU);
-      const bool wx = xOn && (qx.hsL > dry || qx.hsR > dry);
-      const bool wy = yOn && (qy.hsL > dry || qy.hsR > dry);
-      if (__any_sync(0xffffffffu, wx || wy)) {
-        hllc_select(fx.M, fx.N, fx.T, qx.hsL, qx.hsL * qx.nL, qx.hsL * qx.tL,
-                    qx.hsR, qx.hsR * qx.nR, qx.hsR * qx.tR, dry);
-        hllc_select(fy.M, fy.N, fy.T, qy.hsL, qy.hsL * qy.nL, qy.hsL * qy.tL,
-                    qy.hsR, qy.hsR * qy.nR, qy.hsR * qy.tR, dry);
-      }
-      if (xOn) { fx.pL = qx.pL; fx.pR = qx.pR; } else { fx.M = 0; fx.N = 0; fx.T = 0; fx.pL = 0; fx.pR = 0; }
-      if (yOn) { fy.pL = qy.pL; fy.pR = qy.pR; } else { fy.M = 0; fy.N = 0; fy.T = 0; fy.pL = 0; fy.pR = 0; }
+    Face fx = {0, 0, 0, 0, 0};
+    if (j1 >= 2 && j1 < H - 2 && gi >= 1 && gi < W - 2 && c < BX - 1 && j1 >= y0 - 1 && j1 <= y1) {
+      fx = face_flux(b_m1, h_m1, U_m1, V_m1, xsE, xsB, xsU, xsV,
+                     s_b[sr1][c + 1], s_h[sr1][c + 1], s_U[sr1][c + 1], s_V[sr1][c + 1],
+                     s_xs[xsr][0][c + 1], s_xs[xsr][1][c + 1], s_xs[xsr][2][c + 1], s_xs[xsr][3][c + 1],
+                     dry);
     }
     const int fsr = (r + 5) % 3;    // slot of row r-1
     s_fx[fsr][0][c] = fx.M; s_fx[fsr][1][c] = fx.N; s_fx[fsr][2][c] = fx.T;
     s_fx[fsr][3][c] = fx.pL; s_fx[fsr][4][c] = fx.pR;
+    Face fy = {0, 0, 0, 0, 0};
+    const int j2 = r - 2;
+    if (j2 >= 1 && j2 < H - 2 && gi >= 2 && gi < W - 2 && j2 >= y0 - 2 && j2 <= y1) {
+      // lower cell row r-2 (slopes ys*), upper cell row r-1 (slopes ns*); v is normal
+      fy = face_flux(b_m2, h_m2, V_m2, U_m2, ysE, ysB, ysV, ysU,
+                     b_m1, h_m1, V_m1, U_m1, nsE, nsB, nsV, nsU, dry);
+    }
 
     // ---- S4: theta of row r-2 (src/swe.mjs:511-529) -------------------------
     double th = 1;
@@ -807,7 +796,7 @@ __global__ void k_hllc_batch(int n, const double* in, double* out) {
   if (q >= n) return;
   const double* p = in + 7 * q;
   double o0, o1, o2;
-  hllc_select(o0, o1, o2, p[0], p[1], p[2], p[3], p[4], p[5], p[6]);
+  hllc(o0, o1, o2, p[0], p[1], p[2], p[3], p[4], p[5], p[6]);
   out[3 * q] = o0; out[3 * q + 1] = o1; out[3 * q + 2] = o2;
 }
 

@@ -95,75 +95,12 @@ __device__ __forceinline__ void hllc(double& o0, double& o1, double& o2,
   o2 = o0 * (sM >= 0 ? vL : vR);
 }
 
-// The same HLLC without branches: every candidate of the reference's
-// branches is formed with the reference's expressions and the branch
-// conditions select among them, so the result is bit-identical to hllc()
-// whatever the inputs.  Straight-line code lets the scheduler interleave two
-// independent faces; the unused candidates may divide by zero, harmlessly.
-__device__ __forceinline__ void hllc_select(double& o0, double& o1, double& o2,
-                                            double hL, double huL, double hvL,
-                                            double hR, double huR, double hvR, double dry) {
-  const bool wetL = hL > dry, wetR = hR > dry;
-  const double uLq = huL / hL, vLq = hvL / hL, uRq = huR / hR, vRq = hvR / hR;
-  const double uL = wetL ? uLq : 0, vL = wetL ? vLq : 0;
-  const double uR = wetR ? uRq : 0, vR = wetR ? vRq : 0;
-  const double cL = sqrt(SWE_G * jmax(hL, 0)), cR = sqrt(SWE_G * jmax(hR, 0));
-  const double a = (cL + cR) / 2 + (uL - uR) / 4;
-  const double hStar = a * a / SWE_G;
-  const double qLs = sqrt(0.5 * (hStar + hL) * hStar / (hL * hL));
-  const double qRs = sqrt(0.5 * (hStar + hR) * hStar / (hR * hR));
-  const double qL = hStar > hL ? qLs : 1, qR = hStar > hR ? qRs : 1;
-  double sL = uL - cL * qL, sR = uR + cR * qR;                     // wet | wet
-  if (!wetL) { sL = uR - 2 * cR; sR = uR + cR; }                   // dry | wet (selects)
-  else if (!wetR) { sL = uL - cL; sR = uL + 2 * cL; }              // wet | dry
-  const double FL0 = huL, FL1 = huL * uL + 0.5 * SWE_G * hL * hL, FL2 = hvL * uL;
-  const double FR0 = huR, FR1 = huR * uR + 0.5 * SWE_G * hR * hR, FR2 = hvR * uR;
-  const double num = sL * hR * (uR - sR) - sR * hL * (uL - sL);
-  const double den = hR * (uR - sR) - hL * (uL - sL);
-  const double sMq = num / den;
-  const double sM = fabs(den) > 1e-30 ? sMq : 0.5 * (sL + sR);
-  const double inv = 1 / (sR - sL);
-  const double H0 = (sR * FL0 - sL * FR0 + sL * sR * (hR - hL)) * inv;
-  const double H1 = (sR * FL1 - sL * FR1 + sL * sR * (huR - huL)) * inv;
-  const double H2 = H0 * (sM >= 0 ? vL : vR);
-  const bool none = !wetL && !wetR, left = sL >= 0, right = sR <= 0;
-  o0 = none ? 0.0 : left ? FL0 : right ? FR0 : H0;
-  o1 = none ? 0.0 : left ? FL1 : right ? FR1 : H1;
-  o2 = none ? 0.0 : left ? FL2 : right ? FR2 : H2;
-}
-
 // One interface: MUSCL reconstruction from the two cells' slopes along the
 // face normal, Audusse hydrostatic reconstruction against the higher bed,
 // HLLC, and the two interface-local pressure corrections
 // (src/swe.mjs:415-445 for x faces, :448-475 for y faces).  For a y face the
 // caller passes (v, u) as (normal, transverse).
 struct Face { double M, N, T, pL, pR; };
-
-// The reconstructed, hydrostatically re-measured states of one interface
-// (src/swe.mjs:418-435 / 451-465) ahead of the Riemann solve.
-struct FaceState { double hsL, nL, tL, hsR, nR, tR, pL, pR; };
-
-__device__ __forceinline__ FaceState face_state(
-    double bL_c, double hL_c, double nL_c, double tL_c, double sEL, double sBL, double sNL, double sTL,
-    double bR_c, double hR_c, double nR_c, double tR_c, double sER, double sBR, double sNR, double sTR) {
-  const double etaL = bL_c + hL_c + 0.5 * sEL;
-  const double etaR = bR_c + hR_c - 0.5 * sER;
-  const double bL = bL_c + 0.5 * sBL;
-  const double bR = bR_c - 0.5 * sBR;
-  const double hLf = jmax0(etaL - bL);
-  const double hRf = jmax0(etaR - bR);
-  FaceState f;
-  f.nL = nL_c + 0.5 * sNL;
-  f.nR = nR_c - 0.5 * sNR;
-  f.tL = tL_c + 0.5 * sTL;
-  f.tR = tR_c - 0.5 * sTR;
-  const double bStar = jmax(bL, bR);
-  f.hsL = jmax0(etaL - bStar);
-  f.hsR = jmax0(etaR - bStar);
-  f.pL = 0.5 * SWE_G * (hLf * hLf - f.hsL * f.hsL);
-  f.pR = 0.5 * SWE_G * (hRf * hRf - f.hsR * f.hsR);
-  return f;
-}
 
 __device__ __forceinline__ Face face_flux(
     double bL_c, double hL_c, double nL_c, double tL_c,        // left cell b, h, normal vel, transverse vel
