@@ -204,6 +204,23 @@ int swe_hllc_batch(int n, const double* in, double* out);
 /* sim.vel(hq, h) (src/swe.mjs:282) over a batch, on the device. */
 int swe_vel_batch(swe_sim* s, int n, const double* hq, const double* h, double* out);
 
+/* maxDt() for callers that cannot allocate device memory.  It has no
+ * counterpart in the reference; it serves callers that own all device memory
+ * themselves (a fixed arena, a hard memory cap, a region where allocation is
+ * forbidden) and so cannot create a handle.  Inputs are the caller's device
+ * arrays over the padded grid (h, hu, hv: (nx+4)*(ny+4) doubles; dx_row,
+ * dy_cfl: ny+4 doubles, the metric rows of src/geometry.mjs); the result,
+ * cfl / max rate or Infinity, is written to the device double *dt_out, in
+ * `stream` (a cudaStream_t, NULL for the default stream).  It allocates
+ * nothing: its reduction scratch is a fixed array inside the library, so
+ * ny is limited to SWE_NOALLOC_MAX_ROWS (larger grids get SWE_EINVAL), calls
+ * that overlap on the GPU race, and the first call on each device looks the
+ * array up and should come before any stream capture. */
+#define SWE_NOALLOC_MAX_ROWS 16384
+int swe_max_dt_noalloc(int nx, int ny, const double* h, const double* hu, const double* hv,
+                       const double* dx_row, const double* dy_cfl, double min_depth, double cfl,
+                       double* dt_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

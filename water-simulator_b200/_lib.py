@@ -89,6 +89,7 @@ SIGNATURES = {
     "swe_compute_geometry": [ctypes.POINTER(SweOptions), _DP, _DP],
     "swe_hllc_batch": [_I, _DP, _DP],
     "swe_vel_batch": [_P, _I, _DP, _DP, _DP],
+    "swe_max_dt_noalloc": [_I, _I, _P, _P, _P, _P, _P, _D, _D, _P, _P],
 }
 _RESTYPES = {"swe_last_error": ctypes.c_char_p}
 

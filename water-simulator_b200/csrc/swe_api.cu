@@ -44,6 +44,11 @@ double cos_lat(double p) {                                                      
 
 }  // namespace
 
+namespace swe_host {
+// Lets the other translation unit of the library report through swe_last_error().
+void set_error(const std::string& msg) { g_err = msg; }
+}  // namespace swe_host
+
 struct swe_sim {
   swe_options o;
   int nx, ny, W, H, N;
