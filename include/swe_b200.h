@@ -204,6 +204,36 @@ int swe_hllc_batch(int n, const double* in, double* out);
 /* sim.vel(hq, h) (src/swe.mjs:282) over a batch, on the device. */
 int swe_vel_batch(swe_sim* s, int n, const double* hq, const double* h, double* out);
 
+/* ---- Batched ensemble ----------------------------------------------------
+ * Many independent basins of uneven sizes (each a full ShallowWater with its
+ * own options, bed, boundaries, Manning n and Flather tide, and its own dt =
+ * maxDt() every step) advanced together: one launch per kernel per ensemble
+ * step over a tile list of all basins, captured as CUDA graphs.  The
+ * schedule (rows per tile, CTAs -- 0 for one CTA per tile, else a persistent
+ * grid -- and tile order: 0 basin-major, 1 largest basin first, 2 round
+ * robin) is set explicitly or chosen by swe_batch_autotune, which times every
+ * candidate on the ensemble itself and restores the state afterwards.  Each
+ * basin's result is bit-identical to advancing it alone with swe_run.  The
+ * reference drives one basin per ShallowWater (src/swe.mjs:145); this is the
+ * many-basin form of that loop. */
+typedef struct swe_batch swe_batch;
+int swe_batch_create(int n, const swe_options* opts, const double* const* b, const double* const* h,
+                     swe_batch** out);
+int swe_batch_destroy(swe_batch* s);
+int swe_batch_set_boundary(swe_batch* s, int basin, int side, int kind);
+int swe_batch_set_flather_tide(swe_batch* s, int basin, int side, double msl, int n, const double* amp,
+                               const double* omega, const double* phase_deg, double u_coef);
+int swe_batch_set_schedule(swe_batch* s, int rows_per_tile, int ctas, int order);
+/* rows per tile, ctas, order, number of tiles */
+int swe_batch_get_schedule(swe_batch* s, int* out4);
+int swe_batch_autotune(swe_batch* s, int trial_steps, int* best4, double* best_ms_per_step);
+/* `steps` ensemble steps: every basin takes `steps` steps of its own maxDt(). */
+int swe_batch_run(swe_batch* s, int steps);
+int swe_batch_synchronize(swe_batch* s);
+int swe_batch_get_stream(swe_batch* s, void** stream);
+int swe_batch_get_field(swe_batch* s, int basin, int field, double* out);   /* B, H, HU, HV */
+int swe_batch_get_scalar(swe_batch* s, int basin, int which, double* out);  /* T, STEPS, MASS_FLOORED */
+
 /* maxDt() for callers that cannot allocate device memory.  It has no
  * counterpart in the reference; it serves callers that own all device memory
  * themselves (a fixed arena, a hard memory cap, a region where allocation is

@@ -90,6 +90,18 @@ SIGNATURES = {
     "swe_hllc_batch": [_I, _DP, _DP],
     "swe_vel_batch": [_P, _I, _DP, _DP, _DP],
     "swe_max_dt_noalloc": [_I, _I, _P, _P, _P, _P, _P, _D, _D, _P, _P],
+    "swe_batch_create": [_I, ctypes.POINTER(SweOptions), ctypes.POINTER(_DP), ctypes.POINTER(_DP), ctypes.POINTER(_P)],
+    "swe_batch_destroy": [_P],
+    "swe_batch_set_boundary": [_P, _I, _I, _I],
+    "swe_batch_set_flather_tide": [_P, _I, _I, _D, _I, _DP, _DP, _DP, _D],
+    "swe_batch_set_schedule": [_P, _I, _I, _I],
+    "swe_batch_get_schedule": [_P, _IP],
+    "swe_batch_autotune": [_P, _I, _IP, _DP],
+    "swe_batch_run": [_P, _I],
+    "swe_batch_synchronize": [_P],
+    "swe_batch_get_stream": [_P, ctypes.POINTER(_P)],
+    "swe_batch_get_field": [_P, _I, _I, _DP],
+    "swe_batch_get_scalar": [_P, _I, _I, _DP],
 }
 _RESTYPES = {"swe_last_error": ctypes.c_char_p}
 

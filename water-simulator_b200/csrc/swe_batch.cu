@@ -1,0 +1,498 @@
+// swe_batch.cu -- many independent basins of uneven sizes advanced together.
+//
+// Each basin is a complete ShallowWater (its own grid, bed, metric, Manning
+// n, boundaries and Flather tide) with its own dt = maxDt() every step.  One
+// ensemble step is five launches whatever the number of basins:
+//   k_batch_prepare     dt and Flather values of every basin (one thread each)
+//   k_batch_bc(A)       ghost rings of every basin (grid y = basin)
+//   k_batch_stage<1>    every tile of every basin, from one tile list
+//   k_batch_bc(B)
+//   k_batch_stage<2>    ... the last tile of each basin closes that basin's step
+// and a run of steps is captured as a CUDA graph.  The stage kernel is the
+// same tile function as the single-grid kernel, so each basin's result is
+// bit-identical to advancing it alone.  The tile list's row height, the
+// number of CTAs (one per tile, or a persistent grid looping over the list)
+// and the order of the tiles form the schedule, which swe_batch_autotune
+// chooses by timing candidates on the ensemble itself.
+#include "../../include/swe_b200.h"
+#include "swe_kernels.cuh"
+
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace swe_host { void set_error(const std::string& msg); }
+
+namespace {
+
+using swe::BCArgs;
+using swe::Control;
+using swe::PrepArgs;
+using swe::StageArgs;
+
+struct BatchBasin {
+  StageArgs s1, s2;       // stage 1 (A -> B) and stage 2 (B -> A) arguments
+  BCArgs bcA, bcB;
+  Control* ctl;
+  PrepArgs prep;
+};
+
+struct BatchTile { int basin, strip, y0, y1, part; };
+
+__global__ void k_batch_prepare(BatchBasin* basins, int nb) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < nb) swe::prepare_one(basins[q].ctl, basins[q].prep);
+}
+
+__global__ void k_batch_bc(BatchBasin* basins, int which) {
+  const BatchBasin& B = basins[blockIdx.y];
+  if (B.ctl->stop) return;
+  swe::apply_bc_range(which == 0 ? B.bcA : B.bcB, B.ctl, blockIdx.x * blockDim.x + threadIdx.x,
+                      gridDim.x * blockDim.x);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(swe::BX, SWE_STAGE_MIN_BLOCKS)
+k_batch_stage(BatchBasin* basins, const BatchTile* tiles, int ntiles) {
+  extern __shared__ double smem[];
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BatchTile tile = tiles[t];
+    const BatchBasin& B = basins[tile.basin];
+    swe::stage_tile<MODE>(MODE == 1 ? B.s1 : B.s2, B.ctl, tile.strip, tile.y0, tile.y1, tile.part, smem);
+    __syncthreads();          // the next tile reuses the shared rings
+  }
+}
+
+int fail(int code, const std::string& m) { swe_host::set_error(m); return code; }
+
+#define CU(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) return fail(SWE_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+}  // namespace
+
+struct swe_batch {
+  int nb = 0;
+  std::vector<swe_options> opts;
+  std::vector<int> W, H;
+  std::vector<size_t> off;          // per-basin offset (doubles) of its block in the pool
+  std::vector<BatchBasin> host;     // descriptors (device pointers inside)
+  cudaStream_t st = nullptr;
+  double* pool = nullptr;           // all basins' fields, metric rows and partial slots
+  Control* ctls = nullptr;
+  BatchBasin* d_basins = nullptr;
+  BatchTile* d_tiles = nullptr;
+  int ntiles = 0, tile_cap = 0;
+  int rows = 32, ctas = 0, order = 0;   // the schedule
+  int grid = 0;
+  double* save = nullptr;           // autotune snapshot of every basin's A and control
+  size_t save_doubles = 0;
+  cudaGraphExec_t gexec = nullptr;
+  int g_steps = 0;
+  unsigned long long version = 1, g_version = 0;
+};
+
+namespace {
+
+size_t round_up(size_t n) { return (n + 31) & ~size_t(31); }   // 256-byte multiples
+
+// Fill the tile list for the current schedule and upload it.
+int build_tiles(swe_batch* s) {
+  std::vector<std::vector<BatchTile>> per(s->nb);
+  for (int b = 0; b < s->nb; b++) {
+    const int gx = (s->W[b] + swe::SX - 1) / swe::SX;
+    const int gy = (s->H[b] + s->rows - 1) / s->rows;
+    const int ry = (s->H[b] + gy - 1) / gy;
+    int part = 0;
+    for (int y = 0; y < gy; y++)
+      for (int x = 0; x < gx; x++) {
+        const int y0 = y * ry;
+        per[b].push_back({b, x, y0, std::min(y0 + ry, s->H[b]), part++});
+      }
+  }
+  std::vector<int> basin_order(s->nb);
+  std::iota(basin_order.begin(), basin_order.end(), 0);
+  if (s->order == 1)                // largest basins first
+    std::stable_sort(basin_order.begin(), basin_order.end(),
+                     [&](int a, int b) { return (long)s->W[a] * s->H[a] > (long)s->W[b] * s->H[b]; });
+  std::vector<BatchTile> tiles;
+  if (s->order == 2) {              // round robin over basins
+    size_t most = 0;
+    for (auto& v : per) most = std::max(most, v.size());
+    for (size_t k = 0; k < most; k++)
+      for (int b : basin_order)
+        if (k < per[b].size()) tiles.push_back(per[b][k]);
+  } else {
+    for (int b : basin_order) tiles.insert(tiles.end(), per[b].begin(), per[b].end());
+  }
+  s->ntiles = (int)tiles.size();
+  if (s->ntiles > s->tile_cap) {
+    if (s->d_tiles) { cudaStreamSynchronize(s->st); cudaFree(s->d_tiles); s->d_tiles = nullptr; }
+    CU(cudaMalloc(&s->d_tiles, sizeof(BatchTile) * s->ntiles));
+    s->tile_cap = s->ntiles;
+  }
+  CU(cudaMemcpyAsync(s->d_tiles, tiles.data(), sizeof(BatchTile) * s->ntiles, cudaMemcpyHostToDevice, s->st));
+  // partial-slot counts per basin follow the tile count
+  for (int b = 0; b < s->nb; b++) {
+    s->host[b].s1.nblocks = (int)per[b].size();
+    s->host[b].s2.nblocks = (int)per[b].size();
+  }
+  CU(cudaMemcpyAsync(s->d_basins, s->host.data(), sizeof(BatchBasin) * s->nb, cudaMemcpyHostToDevice, s->st));
+  s->grid = s->ctas > 0 ? s->ctas : s->ntiles;
+  CU(cudaStreamSynchronize(s->st));
+  s->version++;
+  return SWE_OK;
+}
+
+int enqueue_batch_step(swe_batch* s) {
+  k_batch_prepare<<<(s->nb + 63) / 64, 64, 0, s->st>>>(s->d_basins, s->nb);
+  CU(cudaGetLastError());
+  int most = 0;
+  for (int b = 0; b < s->nb; b++) most = std::max(most, 4 * s->opts[b].ny + 4 * (s->opts[b].nx + 4));
+  const dim3 bcg((most + 255) / 256, s->nb);
+  k_batch_bc<<<bcg, 256, 0, s->st>>>(s->d_basins, 0);
+  CU(cudaGetLastError());
+  k_batch_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+  CU(cudaGetLastError());
+  k_batch_bc<<<bcg, 256, 0, s->st>>>(s->d_basins, 1);
+  CU(cudaGetLastError());
+  k_batch_stage<2><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+  CU(cudaGetLastError());
+  return SWE_OK;
+}
+
+int run_steps(swe_batch* s, int steps) {
+  const int chunk = 16;
+  if (steps >= chunk && (!s->gexec || s->g_version != s->version || s->g_steps != chunk)) {
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    cudaGraph_t graph;
+    CU(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+    for (int q = 0; q < chunk; q++) {
+      const int rc = enqueue_batch_step(s);
+      if (rc) { cudaStreamEndCapture(s->st, &graph); return rc; }
+    }
+    CU(cudaStreamEndCapture(s->st, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&s->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(SWE_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    s->g_steps = chunk;
+    s->g_version = s->version;
+  }
+  int left = steps;
+  while (left >= chunk) { CU(cudaGraphLaunch(s->gexec, s->st)); left -= chunk; }
+  for (int q = 0; q < left; q++) { const int rc = enqueue_batch_step(s); if (rc) return rc; }
+  return SWE_OK;
+}
+
+// CFL rate of every basin's current state (the step's epilogue keeps it
+// current afterwards).
+__global__ void k_batch_cfl(BatchBasin* basins) {
+  const BatchBasin& B = basins[blockIdx.x];
+  const StageArgs& a = B.s1;
+  __shared__ double sm[32];
+  double m = 0;
+  for (int q = threadIdx.x; q < a.nx * a.ny; q += blockDim.x) {
+    const int j = q / a.nx + 2, i = q % a.nx + 2, k = j * a.W + i;
+    const double hk = a.h[k];
+    if (hk <= a.minDepth) continue;
+    const double cc = sqrt(SWE_G * hk);
+    const double den = swe::vel_den(hk, a.eps4);
+    const double u = fabs(swe::vel_num(a.hu[k], hk) / den), v = fabs(swe::vel_num(a.hv[k], hk) / den);
+    const double sr = (u + cc) / a.m.dxRow[j] + (v + cc) / a.m.dyCFL[j];
+    if (sr > m) m = sr;
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) mm = fmax(mm, sm[w]);
+    B.ctl->next_max = mm;
+  }
+}
+
+void free_batch(swe_batch* s) {
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  if (s->pool) cudaFree(s->pool);
+  if (s->ctls) cudaFree(s->ctls);
+  if (s->d_basins) cudaFree(s->d_basins);
+  if (s->d_tiles) cudaFree(s->d_tiles);
+  if (s->save) cudaFree(s->save);
+  if (s->st) cudaStreamDestroy(s->st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int swe_batch_create(int n, const swe_options* opts, const double* const* b, const double* const* h,
+                     swe_batch** out) {
+  if (!out) return fail(SWE_EINVAL, "null output handle");
+  *out = nullptr;
+  if (n < 1 || !opts || !b || !h) return fail(SWE_EINVAL, "swe_batch_create: n >= 1 basins with options, b and h");
+  swe_batch* s = new swe_batch();
+  auto bail = [&](int rc) { free_batch(s); delete s; return rc; };
+  s->nb = n;
+  s->opts.assign(opts, opts + n);
+  std::vector<std::vector<double>> geom(n);
+  std::vector<double> scal(6);
+  size_t total = 0;
+  for (int q = 0; q < n; q++) {
+    const swe_options& o = opts[q];
+    if (o.nx < 1 || o.ny < 1) return bail(fail(SWE_EINVAL, "basin " + std::to_string(q) + ": nx and ny must be >= 1"));
+    if (o.limiter < 0 || o.limiter > 2) return bail(fail(SWE_EINVAL, "unknown limiter; have minmod,mc,central"));
+    s->W.push_back(o.nx + 4);
+    s->H.push_back(o.ny + 4);
+    geom[q].assign((size_t)(SWE_GEOM_NROWS + 3) * s->H[q], 0.0);
+    int rc = swe_compute_geometry(&o, geom[q].data(), scal.data());
+    if (rc) return bail(rc);
+    for (int r = 0; r < 3; r++) {            // reciprocal rows after the 13 metric rows
+      const int src = r == 0 ? SWE_GEOM_DXROW : r == 1 ? SWE_GEOM_DYROWN : SWE_GEOM_DYROWS;
+      for (int j = 0; j < s->H[q]; j++)
+        geom[q][(size_t)(SWE_GEOM_NROWS + r) * s->H[q] + j] = 1.0 / geom[q][(size_t)src * s->H[q] + j];
+    }
+    const size_t N = (size_t)s->W[q] * s->H[q];
+    s->off.push_back(total);
+    // b, A (3), B (3), metric rows, partial slots (3 x up to one per tile at 4-row tiles)
+    const size_t parts = (size_t)((s->W[q] + swe::SX - 1) / swe::SX) * ((s->H[q] + 3) / 4);
+    total += round_up(N) * 7 + round_up((size_t)(SWE_GEOM_NROWS + 3) * s->H[q]) + round_up(3 * parts);
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+    return bail(fail(SWE_ECUDA, "no CUDA device is available; this library has no CPU path"));
+  if (cudaFuncSetAttribute(k_batch_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, swe::STAGE_SMEM_BYTES) ||
+      cudaFuncSetAttribute(k_batch_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, swe::STAGE_SMEM_BYTES) ||
+      cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) ||
+      cudaMalloc(&s->pool, sizeof(double) * total) ||
+      cudaMalloc(&s->ctls, sizeof(Control) * n) ||
+      cudaMalloc(&s->d_basins, sizeof(BatchBasin) * n))
+    return bail(fail(SWE_ECUDA, std::string("swe_batch_create: ") + cudaGetErrorString(cudaGetLastError())));
+  cudaMemsetAsync(s->ctls, 0, sizeof(Control) * n, s->st);
+  cudaMemsetAsync(s->pool, 0, sizeof(double) * total, s->st);
+  s->host.resize(n);
+  for (int q = 0; q < n; q++) {
+    const swe_options& o = opts[q];
+    const size_t N = (size_t)s->W[q] * s->H[q], rN = round_up(N);
+    double* base = s->pool + s->off[q];
+    double* fb = base;
+    double* A[3] = {base + rN, base + 2 * rN, base + 3 * rN};
+    double* Bf[3] = {base + 4 * rN, base + 5 * rN, base + 6 * rN};
+    double* g = base + 7 * rN;
+    const int Hq = s->H[q];
+    double* parts = g + round_up((size_t)(SWE_GEOM_NROWS + 3) * Hq);
+    const size_t pcap = (size_t)((s->W[q] + swe::SX - 1) / swe::SX) * ((Hq + 3) / 4);
+    cudaMemcpyAsync(fb, b[q], sizeof(double) * N, cudaMemcpyHostToDevice, s->st);
+    cudaMemcpyAsync(A[0], h[q], sizeof(double) * N, cudaMemcpyHostToDevice, s->st);
+    cudaMemcpyAsync(g, geom[q].data(), sizeof(double) * geom[q].size(), cudaMemcpyHostToDevice, s->st);
+    BatchBasin& B = s->host[q];
+    std::memset(&B, 0, sizeof B);
+    StageArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.W = s->W[q]; a.H = Hq; a.nx = o.nx; a.ny = o.ny; a.b = fb;
+    a.m.dxRow = g + SWE_GEOM_DXROW * Hq; a.m.dyRowN = g + SWE_GEOM_DYROWN * Hq;
+    a.m.dyRowS = g + SWE_GEOM_DYROWS * Hq; a.m.dyCFL = g + SWE_GEOM_DYCFL * Hq;
+    a.m.bedPhi = g + SWE_GEOM_BEDPHI * Hq; a.m.geoCoef = g + SWE_GEOM_GEOCOEF * Hq;
+    a.m.fRow = g + SWE_GEOM_FROW * Hq; a.m.tanPhi = g + SWE_GEOM_TANPHI * Hq;
+    a.m.rdxRow = g + (SWE_GEOM_NROWS + 0) * Hq; a.m.rdyRowN = g + (SWE_GEOM_NROWS + 1) * Hq;
+    a.m.rdyRowS = g + (SWE_GEOM_NROWS + 2) * Hq;
+    double Rv = 0;
+    {
+      std::vector<double> sc(6);
+      std::vector<double> tmp((size_t)SWE_GEOM_NROWS * Hq);
+      swe_compute_geometry(&o, tmp.data(), sc.data());
+      Rv = sc[SWE_SCALAR_R];
+    }
+    a.m.R = Rv;
+    a.minDepth = o.min_depth; a.eps4 = std::pow(swe::jmax(o.min_depth, 1e-12), 4.0);
+    a.coriolis = o.coriolis; a.sph = o.sphere; a.order = o.order; a.lim = o.limiter;
+    a.manning = o.manning;
+    a.part_max = parts; a.part_fl1 = parts + pcap; a.part_fl2 = parts + 2 * pcap;
+    B.s1 = a; B.s1.h = A[0]; B.s1.hu = A[1]; B.s1.hv = A[2]; B.s1.oh = Bf[0]; B.s1.ohu = Bf[1]; B.s1.ohv = Bf[2];
+    B.s2 = a; B.s2.h = Bf[0]; B.s2.hu = Bf[1]; B.s2.hv = Bf[2]; B.s2.oh = A[0]; B.s2.ohu = A[1]; B.s2.ohv = A[2];
+    BCArgs bc;
+    bc.nx = o.nx; bc.ny = o.ny; bc.W = s->W[q]; bc.H = Hq;
+    for (int side = 0; side < 4; side++) bc.kind[side] = (o.sphere && side < 2) ? SWE_BC_PERIODIC : SWE_BC_REFLECT;
+    bc.minDepth = o.min_depth; bc.eps4 = a.eps4; bc.b = fb;
+    B.bcA = bc; B.bcA.h = A[0]; B.bcA.hu = A[1]; B.bcA.hv = A[2];
+    B.bcB = bc; B.bcB.h = Bf[0]; B.bcB.hu = Bf[1]; B.bcB.hv = Bf[2];
+    B.ctl = s->ctls + q;
+    B.prep.mode = 1; B.prep.dt_host = 0; B.prep.cfl = o.cfl; B.prep.t_end = INFINITY;
+  }
+  int rc = build_tiles(s);
+  if (rc) return bail(rc);
+  k_batch_cfl<<<n, 256, 0, s->st>>>(s->d_basins);
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s->st) != cudaSuccess)
+    return bail(fail(SWE_ECUDA, "swe_batch_create: initial CFL rate failed"));
+  *out = s;
+  return SWE_OK;
+}
+
+int swe_batch_destroy(swe_batch* s) {
+  if (!s) return SWE_OK;
+  if (s->st) cudaStreamSynchronize(s->st);
+  free_batch(s);
+  delete s;
+  return SWE_OK;
+}
+
+int swe_batch_set_boundary(swe_batch* s, int basin, int side, int kind) {
+  if (!s || basin < 0 || basin >= s->nb || side < 0 || side > 3 || kind < 0 || kind > 3)
+    return fail(SWE_EINVAL, "swe_batch_set_boundary: bad basin, side or kind");
+  s->host[basin].bcA.kind[side] = kind;
+  s->host[basin].bcB.kind[side] = kind;
+  if (kind != SWE_BC_FLATHER) s->host[basin].prep.fl_kind[side] = 0;
+  CU(cudaMemcpyAsync(s->d_basins + basin, &s->host[basin], sizeof(BatchBasin), cudaMemcpyHostToDevice, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_batch_set_flather_tide(swe_batch* s, int basin, int side, double msl, int n, const double* amp,
+                               const double* omega, const double* phase_deg, double u_coef) {
+  if (!s || basin < 0 || basin >= s->nb || side < 0 || side > 3 || n < 0 || n > swe::MAX_TIDE ||
+      (n > 0 && (!amp || !omega || !phase_deg)))
+    return fail(SWE_EINVAL, "swe_batch_set_flather_tide: bad basin, side or table (at most 16 constituents)");
+  Control c;
+  CU(cudaMemcpyAsync(&c, s->ctls + basin, sizeof c, cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  c.tide_n[side] = n; c.tide_msl[side] = msl; c.tide_ucoef[side] = u_coef;
+  for (int q = 0; q < n; q++) {
+    c.tide_amp[side][q] = amp[q]; c.tide_omega[side][q] = omega[q]; c.tide_phase[side][q] = phase_deg[q];
+  }
+  CU(cudaMemcpyAsync(s->ctls + basin, &c, sizeof c, cudaMemcpyHostToDevice, s->st));
+  s->host[basin].bcA.kind[side] = SWE_BC_FLATHER;
+  s->host[basin].bcB.kind[side] = SWE_BC_FLATHER;
+  s->host[basin].prep.fl_kind[side] = 1;
+  CU(cudaMemcpyAsync(s->d_basins + basin, &s->host[basin], sizeof(BatchBasin), cudaMemcpyHostToDevice, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_batch_set_schedule(swe_batch* s, int rows_per_tile, int ctas, int order) {
+  if (!s || rows_per_tile < 4 || rows_per_tile > swe::RY_MAX || ctas < 0 || order < 0 || order > 2)
+    return fail(SWE_EINVAL, "swe_batch_set_schedule: rows in [4, 64], ctas >= 0, order 0..2");
+  s->rows = rows_per_tile; s->ctas = ctas; s->order = order;
+  return build_tiles(s);
+}
+
+int swe_batch_get_schedule(swe_batch* s, int* out4) {
+  if (!s || !out4) return fail(SWE_EINVAL, "null argument");
+  out4[0] = s->rows; out4[1] = s->ctas; out4[2] = s->order; out4[3] = s->ntiles;
+  return SWE_OK;
+}
+
+int swe_batch_run(swe_batch* s, int steps) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (steps <= 0) return SWE_OK;
+  return run_steps(s, steps);
+}
+
+int swe_batch_synchronize(swe_batch* s) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_batch_get_stream(swe_batch* s, void** stream) {
+  if (!s || !stream) return fail(SWE_EINVAL, "null argument");
+  *stream = (void*)s->st;
+  return SWE_OK;
+}
+
+int swe_batch_get_field(swe_batch* s, int basin, int field, double* out) {
+  if (!s || !out || basin < 0 || basin >= s->nb) return fail(SWE_EINVAL, "swe_batch_get_field: bad basin");
+  const BatchBasin& B = s->host[basin];
+  const double* p = field == SWE_FIELD_B ? B.s1.b : field == SWE_FIELD_H ? B.s1.h :
+                    field == SWE_FIELD_HU ? B.s1.hu : field == SWE_FIELD_HV ? B.s1.hv : nullptr;
+  if (!p) return fail(SWE_EINVAL, "swe_batch_get_field: b, h, hu or hv");
+  CU(cudaMemcpyAsync(out, p, sizeof(double) * s->W[basin] * s->H[basin], cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_batch_get_scalar(swe_batch* s, int basin, int which, double* out) {
+  if (!s || !out || basin < 0 || basin >= s->nb) return fail(SWE_EINVAL, "swe_batch_get_scalar: bad basin");
+  Control c;
+  CU(cudaMemcpyAsync(&c, s->ctls + basin, sizeof c, cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  if (which == SWE_SCALAR_T) *out = c.t;
+  else if (which == SWE_SCALAR_STEPS) *out = c.steps;
+  else if (which == SWE_SCALAR_MASS_FLOORED) *out = c.mass_floored;
+  else return fail(SWE_EINVAL, "swe_batch_get_scalar: t, steps or massFloored");
+  return SWE_OK;
+}
+
+int swe_batch_autotune(swe_batch* s, int trial_steps, int* best4, double* best_ms) {
+  if (!s || trial_steps < 1) return fail(SWE_EINVAL, "swe_batch_autotune: trial_steps >= 1");
+  // snapshot every basin's state and control, restored after each trial
+  size_t n = 0;
+  for (int b = 0; b < s->nb; b++) n += 3 * (size_t)s->W[b] * s->H[b];
+  if (!s->save) {
+    CU(cudaMalloc(&s->save, sizeof(double) * n + sizeof(Control) * s->nb));
+    s->save_doubles = n;
+  }
+  auto snapshot = [&](bool restore) -> int {
+    size_t o = 0;
+    for (int b = 0; b < s->nb; b++) {
+      const size_t N = (size_t)s->W[b] * s->H[b];
+      double* f[3] = {s->host[b].s2.oh, s->host[b].s2.ohu, s->host[b].s2.ohv};   // A = (h, hu, hv)
+      for (int q = 0; q < 3; q++) {
+        if (restore) CU(cudaMemcpyAsync(f[q], s->save + o, sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st));
+        else CU(cudaMemcpyAsync(s->save + o, f[q], sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st));
+        o += N;
+      }
+    }
+    Control* cs = reinterpret_cast<Control*>(s->save + s->save_doubles);
+    if (restore) CU(cudaMemcpyAsync(s->ctls, cs, sizeof(Control) * s->nb, cudaMemcpyDeviceToDevice, s->st));
+    else CU(cudaMemcpyAsync(cs, s->ctls, sizeof(Control) * s->nb, cudaMemcpyDeviceToDevice, s->st));
+    return SWE_OK;
+  };
+  int rc = snapshot(false);
+  if (rc) return rc;
+  int dev = 0, sms = 148, occ = 3;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_stage<2>, swe::BX, swe::STAGE_SMEM_BYTES);
+  const int rows_c[] = {16, 24, 32, 48, 64};
+  const int ctas_c[] = {0, sms * std::max(occ, 1), 2 * sms * std::max(occ, 1)};
+  double best = INFINITY;
+  int br = s->rows, bc = s->ctas, bo = s->order;
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  for (int r : rows_c)
+    for (int c : ctas_c)
+      for (int o = 0; o < 3; o++) {
+        s->rows = r; s->ctas = c; s->order = o;
+        rc = build_tiles(s);
+        if (rc) return rc;
+        rc = run_steps(s, 1);                    // warm
+        if (rc) return rc;
+        CU(cudaEventRecord(e0, s->st));
+        rc = run_steps(s, trial_steps);
+        if (rc) return rc;
+        CU(cudaEventRecord(e1, s->st));
+        CU(cudaEventSynchronize(e1));
+        float ms = 0;
+        CU(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) { best = ms; br = r; bc = c; bo = o; }
+        rc = snapshot(true);
+        if (rc) return rc;
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  s->rows = br; s->ctas = bc; s->order = bo;
+  rc = build_tiles(s);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(s->st));
+  if (best4) { best4[0] = br; best4[1] = bc; best4[2] = bo; best4[3] = s->ntiles; }
+  if (best_ms) *best_ms = best / trial_steps;
+  return SWE_OK;
+}
+
+}  // extern "C"

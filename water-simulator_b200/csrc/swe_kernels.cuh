@@ -34,6 +34,7 @@
 #include "swe_math.cuh"
 
 namespace swe {
+namespace {   // every definition here is private to the including translation unit
 
 constexpr int BX = 128;          // threads per CTA = columns per strip incl. halos
 constexpr int HALO = 4;          // halo columns each side (left edge stays 16-byte aligned)
@@ -105,8 +106,7 @@ struct PrepArgs {
   double fl_eta[4], fl_u[4];
 };
 
-__global__ void k_prepare(Control* ctl, PrepArgs a) {
-  if (threadIdx.x != 0) return;
+__device__ __forceinline__ void prepare_one(Control* ctl, const PrepArgs& a) {
   double dt;
   if (a.mode == 0) dt = a.dt_host;
   else if (a.mode == 2) dt = jmin(a.dt_host, a.t_end - ctl->t);
@@ -130,6 +130,10 @@ __global__ void k_prepare(Control* ctl, PrepArgs a) {
       ctl->fl_u[s] = a.fl_u[s];
     }
   }
+}
+
+__global__ void k_prepare(Control* ctl, PrepArgs a) {
+  if (threadIdx.x == 0) prepare_one(ctl, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -221,11 +225,11 @@ __device__ Cell sn_ghost(const BCArgs& a, const Control* ctl, int i, int j) {
   return flather_cell(a, ctl, side, load_cell(a, clampi(i, 0, a.nx - 1), clampi(j, 0, a.ny - 1)));
 }
 
-__global__ void k_apply_bc(BCArgs a, const Control* ctl, int respect_stop) {
-  if (respect_stop && ctl->stop) return;
+// Ghost cells q0, q0 + stride, ... of one grid.
+__device__ __forceinline__ void apply_bc_range(const BCArgs& a, const Control* ctl, int q0, int stride) {
   const int nwe = 4 * a.ny;                 // 2 sides x 2 rings x ny interior rows
   const int nsn = 4 * (a.nx + 4);           // 2 sides x 2 rings x (nx + 4) columns
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nwe + nsn; q += gridDim.x * blockDim.x) {
+  for (int q = q0; q < nwe + nsn; q += stride) {
     int i, j;
     Cell c;
     if (q < nwe) {
@@ -245,6 +249,11 @@ __global__ void k_apply_bc(BCArgs a, const Control* ctl, int respect_stop) {
   }
 }
 
+__global__ void k_apply_bc(BCArgs a, const Control* ctl, int respect_stop) {
+  if (respect_stop && ctl->stop) return;
+  apply_bc_range(a, ctl, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 // ---------------------------------------------------------------------------
 // Fused residual + stage update.  MODE 0: residual only (rh, rhu, rhv,
 // theta for every cell, src/swe.mjs:308-629); MODE 1: stage 1
@@ -259,12 +268,15 @@ constexpr int STAGE_SMEM_BYTES = (49 * BX + M_COUNT * MROWS) * 8;
 #ifndef SWE_STAGE_MIN_BLOCKS
 #define SWE_STAGE_MIN_BLOCKS 3
 #endif
+// One tile: output columns strip*SX .. +SX (padded), output rows [y0, y1).
+// `part` is this tile's slot among the `a.nblocks` partial slots of its grid,
+// whose last finisher closes the step.  Every thread of the CTA calls it.
 template <int MODE>
-__global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a, Control* ctl) {
+__device__ __forceinline__ void stage_tile(const StageArgs& a, Control* ctl, int strip, int y0, int y1,
+                                           int part, double* smem) {
   if (MODE != 0 && ctl->stop) return;
   // state ring, 4 rows deep: b, h, U, V are read by neighbours (rows r-1),
   // h, hu, hv, U of row r-3 by the cell's own thread in S5
-  extern __shared__ double smem[];                                   // STAGE_SMEM_BYTES
   double (*s_b)[BX] = reinterpret_cast<double (*)[BX]>(smem);
   double (*s_h)[BX] = s_b + 4;
   double (*s_U)[BX] = s_b + 8;
@@ -279,11 +291,9 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
 
   const int c = threadIdx.x;
   const int W = a.W, H = a.H;
-  const int gi = (int)blockIdx.x * SX - HALO + c;
+  const int gi = strip * SX - HALO + c;
   const bool colIn = gi >= 0 && gi < W;
-  const int RY = (H + gridDim.y - 1) / gridDim.y;     // <= RY_MAX (host)
-  const int y0 = (int)blockIdx.y * RY;
-  const int y1 = min(y0 + RY, H);            // output rows [y0, y1)
+  const int RY = y1 - y0;                    // <= RY_MAX (host)
   const int mbase = y0 - 3;                  // metric row m = j - mbase
   const double dt = ctl->dt;
   const double dry = a.minDepth, eps4 = a.eps4;
@@ -593,7 +603,7 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
     if ((c & 31) == 0) { s_red[0][c >> 5] = locMax; s_red[1][c >> 5] = locFl; }
     __syncthreads();
     __shared__ bool s_last;
-    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    const int bid = part;
     if (c == 0) {
       double m = s_red[0][0], f = s_red[1][0];
       for (int w = 1; w < BX / 32; w++) { m = fmax(m, s_red[0][w]); f += s_red[1][w]; }
@@ -625,6 +635,15 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
       ctl->counter = 0;
     }
   }
+}
+
+// The single-grid stage kernel: a 2D grid of tiles over one simulation.
+template <int MODE>
+__global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a, Control* ctl) {
+  extern __shared__ double smem[];                                   // STAGE_SMEM_BYTES
+  const int RY = (a.H + gridDim.y - 1) / gridDim.y;
+  const int y0 = (int)blockIdx.y * RY;
+  stage_tile<MODE>(a, ctl, blockIdx.x, y0, min(y0 + RY, a.H), blockIdx.y * gridDim.x + blockIdx.x, smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -806,4 +825,5 @@ __global__ void k_vel_batch(int n, const double* hq, const double* h, double eps
   out[q] = vel(hq[q], h[q], eps4);
 }
 
+}  // namespace
 }  // namespace swe

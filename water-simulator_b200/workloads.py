@@ -77,3 +77,26 @@ def bump_dam_break(nx=256, ny=256, dx=5.0, seed=1, still=False):
     X, _ = _centres(nx, ny, dx)
     eta = np.full_like(X, 2.0) if still else np.where(X < nx * dx / 2, 2.0, 0.5)
     return b, eta
+
+
+def ensemble(n=256, seed=4, dx=5.0, amp=0.5, eta=2.0):
+    """The batched-ensemble workload: n independent Cartesian basins of
+    seeded uneven sizes, nx ~ U[64, 1024], ny ~ U[64, 512], each with its own
+    bump-and-roughness bed (seeded per basin), still water at eta = 2 m,
+    Manning n ~ U[0.015, 0.04] and a west Flather tide of amplitude 0.5 m
+    (not given by the configuration; stated here) and period ~ U[2, 14] h.
+    Returns a list of dicts: nx, ny, dx, b, eta0, manning, tide (msl, amp,
+    omega, phase_deg)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        nx = int(rng.integers(64, 1025))
+        ny = int(rng.integers(64, 513))
+        manning = float(rng.uniform(0.015, 0.04))
+        period_h = float(rng.uniform(2.0, 14.0))
+        b = bump_bed(nx, ny, dx, seed=1000 + q)
+        out.append({"nx": nx, "ny": ny, "dx": dx, "b": b, "eta0": np.full_like(b, eta),
+                    "manning": manning,
+                    "tide": {"msl": eta, "amp": [amp], "omega": [2 * math.pi / (period_h * 3600)],
+                             "phase_deg": [0.0]}})
+    return out
