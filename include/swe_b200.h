@@ -234,6 +234,30 @@ int swe_batch_get_stream(swe_batch* s, void** stream);
 int swe_batch_get_field(swe_batch* s, int basin, int field, double* out);   /* B, H, HU, HV */
 int swe_batch_get_scalar(swe_batch* s, int basin, int which, double* out);  /* T, STEPS, MASS_FLOORED */
 
+/* ---- Discrete adjoint ------------------------------------------------------
+ * Gradient of a gauge misfit J = sum_steps sum_gauges (eta - obs)^2 with
+ * respect to the bed b and the per-cell Manning n (both over the padded
+ * grid; ghosts get 0), for `steps` self-timed steps from still water eta0
+ * (h = max(0, eta0 - b), src/swe.mjs:229-231).  Cartesian, walls on every
+ * side.  The forward pass records dt and checkpoints the state every
+ * `checkpoint_every` steps; swe_adjoint_backward recomputes each segment
+ * and runs the hand-written reverse of every step, branches fixed as taken.
+ * gauge_cells are padded indices k = j*W + i.  manning_field may be NULL
+ * (scalar o->manning, no n gradient). */
+typedef struct swe_adjoint swe_adjoint;
+int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0, const double* manning_field,
+                       int n_gauges, const int* gauge_cells, int steps, int checkpoint_every, swe_adjoint** out);
+int swe_adjoint_destroy(swe_adjoint* s);
+int swe_adjoint_set_observations(swe_adjoint* s, const double* obs);      /* steps x n_gauges */
+/* J, and (optional) eta at the gauges after every step (steps x n_gauges). */
+int swe_adjoint_forward(swe_adjoint* s, double* J, double* gauge_eta);
+int swe_adjoint_backward(swe_adjoint* s, double* grad_b, double* grad_n);
+/* The dt of every step (steps doubles): read the sequence of the last
+ * forward pass into dts_out, and/or hold the forward to dts_in from now on
+ * (a finite-difference check needs the same frozen dts). */
+int swe_adjoint_dt_sequence(swe_adjoint* s, double* dts_out, const double* dts_in);
+int swe_adjoint_get_stream(swe_adjoint* s, void** stream);
+
 /* maxDt() for callers that cannot allocate device memory.  It has no
  * counterpart in the reference; it serves callers that own all device memory
  * themselves (a fixed arena, a hard memory cap, a region where allocation is

@@ -42,74 +42,130 @@ const double INF = INFINITY;
 
 thread_local std::string g_err;
 
+// A dual number: a value and its derivative along one direction.  Running
+// the solver on Duals is its tangent-linear model; every comparison looks at
+// the value only, so every branch is the branch the value takes.
+struct Dual {
+  double v, d;
+  Dual(double x = 0) : v(x), d(0) {}
+  Dual(double x, double dx) : v(x), d(dx) {}
+};
+inline Dual operator+(const Dual& a, const Dual& b) { return {a.v + b.v, a.d + b.d}; }
+inline Dual operator-(const Dual& a, const Dual& b) { return {a.v - b.v, a.d - b.d}; }
+inline Dual operator*(const Dual& a, const Dual& b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+inline Dual operator/(const Dual& a, const Dual& b) {
+  const double q = a.v / b.v;
+  return {q, (a.d - q * b.d) / b.v};
+}
+inline Dual operator-(const Dual& a) { return {-a.v, -a.d}; }
+inline Dual operator+(const Dual& a, double b) { return {a.v + b, a.d}; }
+inline Dual operator+(double a, const Dual& b) { return {a + b.v, b.d}; }
+inline Dual operator-(const Dual& a, double b) { return {a.v - b, a.d}; }
+inline Dual operator-(double a, const Dual& b) { return {a - b.v, -b.d}; }
+inline Dual operator*(const Dual& a, double b) { return {a.v * b, a.d * b}; }
+inline Dual operator*(double a, const Dual& b) { return {a * b.v, a * b.d}; }
+inline Dual operator/(const Dual& a, double b) { return {a.v / b, a.d / b}; }
+inline Dual operator/(double a, const Dual& b) { const double q = a / b.v; return {q, -q * b.d / b.v}; }
+inline Dual& operator+=(Dual& a, const Dual& b) { a = a + b; return a; }
+inline Dual& operator-=(Dual& a, const Dual& b) { a = a - b; return a; }
+inline Dual& operator/=(Dual& a, const Dual& b) { a = a / b; return a; }
+#define DUAL_CMP(op)                                                                 \
+  inline bool operator op(const Dual& a, const Dual& b) { return a.v op b.v; }       \
+  inline bool operator op(const Dual& a, double b) { return a.v op b; }              \
+  inline bool operator op(double a, const Dual& b) { return a op b.v; }
+DUAL_CMP(<) DUAL_CMP(>) DUAL_CMP(<=) DUAL_CMP(>=) DUAL_CMP(==) DUAL_CMP(!=)
+#undef DUAL_CMP
+inline double value(double x) { return x; }
+inline double value(const Dual& x) { return x.v; }
+inline double sqrtT(double x) { return std::sqrt(x); }
+inline Dual sqrtT(const Dual& x) { const double r = std::sqrt(x.v); return {r, x.d == 0 ? 0 : x.d / (2 * r)}; }
+inline double fabsT(double x) { return std::fabs(x); }
+inline Dual fabsT(const Dual& x) { return std::signbit(x.v) ? -x : x; }
+inline double hypotT(double a, double b) { return std::hypot(a, b); }
+inline Dual hypotT(const Dual& a, const Dual& b) {
+  const double r = std::hypot(a.v, b.v);
+  return {r, r == 0 ? 0 : (a.v * a.d + b.v * b.d) / r};
+}
+inline double powT(double x, double p) { return std::pow(x, p); }
+inline Dual powT(const Dual& x, double p) {
+  const double r = std::pow(x.v, p);
+  return {r, x.d == 0 ? 0 : p * std::pow(x.v, p - 1) * x.d};
+}
+inline bool isfiniteT(double x) { return std::isfinite(x); }
+inline bool isfiniteT(const Dual& x) { return std::isfinite(x.v); }
+
 // JavaScript Math.max / Math.min semantics: NaN if any operand is NaN, and
 // +0 > -0.  (C fmax/fmin drop NaN operands, which would hide a blow-up.)
-inline double jmax(double a, double b) {
+template <class T> inline T jmaxT(const T& a, const T& b) {
   if (a != a) return a;
   if (b != b) return b;
   if (a > b) return a;
   if (b > a) return b;
-  return std::signbit(a) ? b : a;
+  return std::signbit(value(a)) ? b : a;
 }
-inline double jmin(double a, double b) {
+template <class T> inline T jminT(const T& a, const T& b) {
   if (a != a) return a;
   if (b != b) return b;
   if (a < b) return a;
   if (b < a) return b;
-  return std::signbit(a) ? a : b;
+  return std::signbit(value(a)) ? a : b;
 }
+inline double jmax(double a, double b) { return jmaxT<double>(a, b); }
+inline Dual jmax(const Dual& a, const Dual& b) { return jmaxT<Dual>(a, b); }
+inline double jmin(double a, double b) { return jminT<double>(a, b); }
+inline Dual jmin(const Dual& a, const Dual& b) { return jminT<Dual>(a, b); }
 
 // src/swe.mjs:88-92
-inline double lim_minmod(double a, double b) {
+template <class T> inline T lim_minmod(const T& a, const T& b) {
   if (a > 0 && b > 0) return a < b ? a : b;
   if (a < 0 && b < 0) return a > b ? a : b;
-  return 0;
+  return T(0);
 }
 // src/swe.mjs:133-138
-inline double lim_mc(double a, double b) {
-  if (a * b <= 0) return 0;
-  const double c = 0.5 * (a + b);
-  const double m = jmin(jmin(std::fabs(c), 2 * std::fabs(a)), 2 * std::fabs(b));
+template <class T> inline T lim_mc(const T& a, const T& b) {
+  if (a * b <= 0) return T(0);
+  const T c = 0.5 * (a + b);
+  const T m = jmin(jmin(fabsT(c), 2 * fabsT(a)), 2 * fabsT(b));
   return a > 0 ? m : -m;
 }
 // src/swe.mjs:141
-inline double lim_central(double a, double b) { return 0.5 * (a + b); }
+template <class T> inline T lim_central(const T& a, const T& b) { return 0.5 * (a + b); }
 
 // src/swe.mjs:1013-1018
-inline void flux1D(double* out, double h, double hu, double hv, double u) {
+template <class T> inline void flux1D(T* out, const T& h, const T& hu, const T& hv, const T& u) {
   out[0] = hu;
   out[1] = hu * u + 0.5 * G * h * h;
   out[2] = hv * u;
 }
 
 // src/swe.mjs:975-1011
-void hllc(double* out, double hL, double huL, double hvL, double hR, double huR, double hvR,
-          double dry) {
+template <class T>
+void hllc(T* out, T hL, T huL, T hvL, T hR, T huR, T hvR, double dry) {
   const bool wetL = hL > dry, wetR = hR > dry;
-  if (!wetL && !wetR) { out[0] = out[1] = out[2] = 0; return; }
-  const double uL = wetL ? huL / hL : 0, vL = wetL ? hvL / hL : 0;
-  const double uR = wetR ? huR / hR : 0, vR = wetR ? hvR / hR : 0;
-  const double cL = std::sqrt(G * jmax(hL, 0)), cR = std::sqrt(G * jmax(hR, 0));
-  double sL, sR;
+  if (!wetL && !wetR) { out[0] = out[1] = out[2] = T(0); return; }
+  const T uL = wetL ? huL / hL : T(0), vL = wetL ? hvL / hL : T(0);
+  const T uR = wetR ? huR / hR : T(0), vR = wetR ? hvR / hR : T(0);
+  const T cL = sqrtT(G * jmax(hL, T(0))), cR = sqrtT(G * jmax(hR, T(0)));
+  T sL, sR;
   if (!wetL) { sL = uR - 2 * cR; sR = uR + cR; }
   else if (!wetR) { sL = uL - cL; sR = uL + 2 * cL; }
   else {
-    const double a = (cL + cR) / 2 + (uL - uR) / 4;
-    const double hStar = a * a / G;
-    const double qL = hStar > hL ? std::sqrt(0.5 * (hStar + hL) * hStar / (hL * hL)) : 1;
-    const double qR = hStar > hR ? std::sqrt(0.5 * (hStar + hR) * hStar / (hR * hR)) : 1;
+    const T a = (cL + cR) / 2 + (uL - uR) / 4;
+    const T hStar = a * a / G;
+    const T qL = hStar > hL ? sqrtT(0.5 * (hStar + hL) * hStar / (hL * hL)) : T(1);
+    const T qR = hStar > hR ? sqrtT(0.5 * (hStar + hR) * hStar / (hR * hR)) : T(1);
     sL = uL - cL * qL;
     sR = uR + cR * qR;
   }
   if (sL >= 0) { flux1D(out, hL, huL, hvL, uL); return; }
   if (sR <= 0) { flux1D(out, hR, huR, hvR, uR); return; }
-  const double num = sL * hR * (uR - sR) - sR * hL * (uL - sL);
-  const double den = hR * (uR - sR) - hL * (uL - sL);
-  const double sM = std::fabs(den) > 1e-30 ? num / den : 0.5 * (sL + sR);
-  double FL[3], FR[3];
+  const T num = sL * hR * (uR - sR) - sR * hL * (uL - sL);
+  const T den = hR * (uR - sR) - hL * (uL - sL);
+  const T sM = fabsT(den) > 1e-30 ? num / den : 0.5 * (sL + sR);
+  T FL[3], FR[3];
   flux1D(FL, hL, huL, hvL, uL);
   flux1D(FR, hR, huR, hvR, uR);
-  const double inv = 1 / (sR - sL);
+  const T inv = 1 / (sR - sL);
   out[0] = (sR * FL[0] - sL * FR[0] + sL * sR * (hR - hL)) * inv;
   out[1] = (sR * FL[1] - sL * FR[1] + sL * sR * (huR - huL)) * inv;
   out[2] = out[0] * (sM >= 0 ? vL : vR);
@@ -136,7 +192,8 @@ struct Tide {                 // src/tide.mjs:103-107 as a table
 
 }  // namespace
 
-struct oracle_sim {
+template <class T>
+struct SimT {
   int nx, ny, ng, W, H, N;
   double dx, dy, manning, minDepth, cfl, coriolis, eps4;
   int order, limiter, sphere;
@@ -144,9 +201,9 @@ struct oracle_sim {
   std::vector<double> g[OG_NROWS];
   double R, dlam, dphi, totalArea, lat0, lat1, omega;
   // state and scratch, src/swe.mjs:200-220
-  std::vector<double> b, h, hu, hv, h0, hu0, hv0, rh, rhu, rhv, sE, sU, sV, sB;
-  std::vector<double> fxM, fxN, fxT, fyM, fyN, fyT, pxL, pxR, pyL, pyR, theta, uu, vv;
-  std::vector<double> manningField;
+  std::vector<T> b, h, hu, hv, h0, hu0, hv0, rh, rhu, rhv, sE, sU, sV, sB;
+  std::vector<T> fxM, fxN, fxT, fyM, fyN, fyT, pxL, pxR, pyL, pyR, theta, uu, vv;
+  std::vector<T> manningField;
   bool hasManning = false;
   int bc[4] = {OB_REFLECT, OB_REFLECT, OB_REFLECT, OB_REFLECT};
   double flEta[4] = {0, 0, 0, 0}, flU[4] = {0, 0, 0, 0};
@@ -156,17 +213,18 @@ struct oracle_sim {
   bool hasSponge = false;
   double spongeRef = 0;
   std::vector<std::pair<int, double>> spongeCells;
-  double t = 0, steps = 0, massFloored = 0;
+  double t = 0, steps = 0;
+  T massFloored = 0;
   int threads = 1;
 
   int idx(int i, int j) const { return (j + ng) * W + (i + ng); }
 
   // src/swe.mjs:282-285
-  double vel(double hq, double hh) const {
-    const double h4 = hh * hh * hh * hh;
-    return (SQRT2 * hh * hq) / std::sqrt(h4 + jmax(h4, eps4));
+  T vel(T hq, T hh) const {
+    const T h4 = hh * hh * hh * hh;
+    return (SQRT2 * hh * hq) / sqrtT(h4 + jmax(h4, eps4));
   }
-  double limit(double a, double c) const {
+  T limit(T a, T c) const {
     return limiter == 0 ? lim_mc(a, c) : limiter == 1 ? lim_minmod(a, c) : lim_central(a, c);
   }
 
@@ -195,20 +253,20 @@ struct oracle_sim {
     const int sj = std::max(0, std::min(ny - 1, j));
     const int gk = idx(i, j), s = idx(si, sj);
     b[gk] = b[s];
-    const double bed = b[gk];
-    const double hInt = h[s];
+    const T bed = b[gk];
+    const T hInt = h[s];
     double e0, u0;
     if (flTide[side]) { e0 = tide[side].eta(t); u0 = tide[side].u_coef * tide[side].eta(t); }
     else { e0 = flEta[side]; u0 = flU[side]; }
     if (hInt <= minDepth) { h[gk] = jmax(0, e0 - bed); hu[gk] = 0; hv[gk] = 0; return; }
-    const double etaInt = bed + hInt;
-    const double r = std::sqrt(G / hInt);
+    const T etaInt = bed + hInt;
+    const T r = sqrtT(G / hInt);
     const double sgn = (side == 0 || side == 2) ? 1 : -1;
-    const double uInt = (side == 0 || side == 1) ? vel(hu[s], hInt) : vel(hv[s], hInt);
-    const double Rin = u0 + sgn * e0 * r;
-    const double Rout = uInt - sgn * etaInt * r;
-    const double un = 0.5 * (Rin + Rout);
-    const double en = sgn * (Rin - Rout) / (2 * r);
+    const T uInt = (side == 0 || side == 1) ? vel(hu[s], hInt) : vel(hv[s], hInt);
+    const T Rin = u0 + sgn * e0 * r;
+    const T Rout = uInt - sgn * etaInt * r;
+    const T un = 0.5 * (Rin + Rout);
+    const T en = sgn * (Rin - Rout) / (2 * r);
     h[gk] = jmax(0, en - bed);
     if (side == 0 || side == 1) { hu[gk] = h[gk] * un; hv[gk] = hv[s]; }
     else { hv[gk] = h[gk] * un; hu[gk] = hu[s]; }
@@ -249,7 +307,7 @@ struct oracle_sim {
     const std::vector<double>& dyRowS = g[OG_DYROWS];
     const std::vector<double>& bedPhi = g[OG_BEDPHI];
     const bool sph = sphere != 0;
-    const int T = threads;
+    const int nthr = threads;
     std::fill(rh.begin(), rh.end(), 0.0);
     std::fill(rhu.begin(), rhu.end(), 0.0);
     std::fill(rhv.begin(), rhv.end(), 0.0);
@@ -257,18 +315,18 @@ struct oracle_sim {
     std::fill(fyM.begin(), fyM.end(), 0.0);
 
     // cell velocities, src/swe.mjs:358-359
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
-    for (int k = 0; k < N; k++) { const double hk = h[k]; uu[k] = vel(hu[k], hk); vv[k] = vel(hv[k], hk); }
-    const double* U = uu.data();
-    const double* V = vv.data();
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
+    for (int k = 0; k < N; k++) { const T hk = h[k]; uu[k] = vel(hu[k], hk); vv[k] = vel(hv[k], hk); }
+    const T* U = uu.data();
+    const T* V = vv.data();
 
     // slopes, src/swe.mjs:362-411
     if (order >= 2) {
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
       for (int j = 1; j < H - 1; j++) {
         for (int i = 1; i < W - 1; i++) {
           const int k = j * W + i, k2 = 2 * k;
-          const double hk = h[k], bk = b[k], eC = bk + hk, uk = U[k], vk = V[k];
+          const T hk = h[k], bk = b[k], eC = bk + hk, uk = U[k], vk = V[k];
           for (int d = 0; d < 2; d++) {
             const int kp = d == 0 ? k + 1 : k + W;
             const int km = d == 0 ? k - 1 : k - W;
@@ -276,7 +334,7 @@ struct oracle_sim {
               sE[k2 + d] = 0; sB[k2 + d] = 0; sU[k2 + d] = 0; sV[k2 + d] = 0;
               continue;
             }
-            const double eP = b[kp] + h[kp], eM = b[km] + h[km];
+            const T eP = b[kp] + h[kp], eM = b[km] + h[km];
             sE[k2 + d] = limit(eC - eM, eP - eC);
             sB[k2 + d] = limit(bk - b[km], b[kp] - bk);
             sU[k2 + d] = limit(uk - U[km], U[kp] - uk);
@@ -290,54 +348,54 @@ struct oracle_sim {
     }
 
     // x interfaces, src/swe.mjs:414-445
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
     for (int j = ng; j < H - ng; j++) {
-      double flux[3];
+      T flux[3];
       for (int i = ng - 1; i < W - ng; i++) {
         const int kL = j * W + i, kR = kL + 1, kL2 = 2 * kL, kR2 = 2 * kR;
-        const double etaL = b[kL] + h[kL] + 0.5 * sE[kL2];
-        const double etaR = b[kR] + h[kR] - 0.5 * sE[kR2];
-        const double bL = b[kL] + 0.5 * sB[kL2];
-        const double bR = b[kR] - 0.5 * sB[kR2];
-        const double hLf = jmax(0, etaL - bL);
-        const double hRf = jmax(0, etaR - bR);
-        const double uL = U[kL] + 0.5 * sU[kL2];
-        const double uR = U[kR] - 0.5 * sU[kR2];
-        const double vL = V[kL] + 0.5 * sV[kL2];
-        const double vR = V[kR] - 0.5 * sV[kR2];
-        const double bStar = jmax(bL, bR);
-        const double hsL = jmax(0, etaL - bStar);
-        const double hsR = jmax(0, etaR - bStar);
+        const T etaL = b[kL] + h[kL] + 0.5 * sE[kL2];
+        const T etaR = b[kR] + h[kR] - 0.5 * sE[kR2];
+        const T bL = b[kL] + 0.5 * sB[kL2];
+        const T bR = b[kR] - 0.5 * sB[kR2];
+        const T hLf = jmax(0, etaL - bL);
+        const T hRf = jmax(0, etaR - bR);
+        const T uL = U[kL] + 0.5 * sU[kL2];
+        const T uR = U[kR] - 0.5 * sU[kR2];
+        const T vL = V[kL] + 0.5 * sV[kL2];
+        const T vR = V[kR] - 0.5 * sV[kR2];
+        const T bStar = jmax(bL, bR);
+        const T hsL = jmax(0, etaL - bStar);
+        const T hsR = jmax(0, etaR - bStar);
         hllc(flux, hsL, hsL * uL, hsL * vL, hsR, hsR * uR, hsR * vR, minDepth);
-        const double pL = 0.5 * G * (hLf * hLf - hsL * hsL);
-        const double pR = 0.5 * G * (hRf * hRf - hsR * hsR);
+        const T pL = 0.5 * G * (hLf * hLf - hsL * hsL);
+        const T pR = 0.5 * G * (hRf * hRf - hsR * hsR);
         fxM[kL] = flux[0]; fxN[kL] = flux[1]; fxT[kL] = flux[2];
         pxL[kL] = pL; pxR[kL] = pR;
       }
     }
 
     // y interfaces, src/swe.mjs:447-475
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
     for (int j = ng - 1; j < H - ng; j++) {
-      double flux[3];
+      T flux[3];
       for (int i = ng; i < W - ng; i++) {
         const int kL = j * W + i, kR = kL + W, kL2 = 2 * kL + 1, kR2 = 2 * kR + 1;
-        const double etaL = b[kL] + h[kL] + 0.5 * sE[kL2];
-        const double etaR = b[kR] + h[kR] - 0.5 * sE[kR2];
-        const double bL = b[kL] + 0.5 * sB[kL2];
-        const double bR = b[kR] - 0.5 * sB[kR2];
-        const double hLf = jmax(0, etaL - bL);
-        const double hRf = jmax(0, etaR - bR);
-        const double uL = U[kL] + 0.5 * sU[kL2];
-        const double uR = U[kR] - 0.5 * sU[kR2];
-        const double vL = V[kL] + 0.5 * sV[kL2];
-        const double vR = V[kR] - 0.5 * sV[kR2];
-        const double bStar = jmax(bL, bR);
-        const double hsL = jmax(0, etaL - bStar);
-        const double hsR = jmax(0, etaR - bStar);
+        const T etaL = b[kL] + h[kL] + 0.5 * sE[kL2];
+        const T etaR = b[kR] + h[kR] - 0.5 * sE[kR2];
+        const T bL = b[kL] + 0.5 * sB[kL2];
+        const T bR = b[kR] - 0.5 * sB[kR2];
+        const T hLf = jmax(0, etaL - bL);
+        const T hRf = jmax(0, etaR - bR);
+        const T uL = U[kL] + 0.5 * sU[kL2];
+        const T uR = U[kR] - 0.5 * sU[kR2];
+        const T vL = V[kL] + 0.5 * sV[kL2];
+        const T vR = V[kR] - 0.5 * sV[kR2];
+        const T bStar = jmax(bL, bR);
+        const T hsL = jmax(0, etaL - bStar);
+        const T hsR = jmax(0, etaR - bStar);
         hllc(flux, hsL, hsL * vL, hsL * uL, hsR, hsR * vR, hsR * uR, minDepth);
-        const double pL = 0.5 * G * (hLf * hLf - hsL * hsL);
-        const double pR = 0.5 * G * (hRf * hRf - hsR * hsR);
+        const T pL = 0.5 * G * (hLf * hLf - hsL * hsL);
+        const T pR = 0.5 * G * (hRf * hRf - hsR * hsR);
         fyM[kL] = flux[0]; fyN[kL] = flux[1]; fyT[kL] = flux[2];
         pyL[kL] = pL; pyR[kL] = pR;
       }
@@ -346,28 +404,28 @@ struct oracle_sim {
     // positivity limiter, src/swe.mjs:511-529
     std::fill(theta.begin(), theta.end(), 1.0);
     if (dt > 0) {
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
       for (int j = ng - 1; j < H - ng + 1; j++) {
         for (int i = ng - 1; i < W - ng + 1; i++) {
           const int k = j * W + i;
-          double out = 0;
+          T out = 0;
           if (fxM[k] > 0) out += fxM[k] / dxRow[j];
           if (fxM[k - 1] < 0) out -= fxM[k - 1] / dxRow[j];
           if (fyM[k] > 0) out += fyM[k] / dyRowN[j];
           if (fyM[k - W] < 0) out -= fyM[k - W] / dyRowS[j];
-          const double avail = h[k];
+          const T avail = h[k];
           if (out * dt > avail) theta[k] = avail > 0 ? avail / (out * dt) : 0;
         }
       }
     }
 
-    if (T <= 1) {
+    if (nthr <= 1) {
       // accumulate, src/swe.mjs:530-555, as the reference's scatter loops
       for (int j = ng; j < H - ng; j++) {
         for (int i = ng - 1; i < W - ng; i++) {
           const int kL = j * W + i, kR = kL + 1;
-          const double th = fxM[kL] >= 0 ? theta[kL] : theta[kR];
-          const double inv = th / dxRow[j];
+          const T th = fxM[kL] >= 0 ? theta[kL] : theta[kR];
+          const T inv = th / dxRow[j];
           rh[kL] -= fxM[kL] * inv; rhu[kL] -= (fxN[kL] + pxL[kL]) * inv; rhv[kL] -= fxT[kL] * inv;
           rh[kR] += fxM[kL] * inv; rhu[kR] += (fxN[kL] + pxR[kL]) * inv; rhv[kR] += fxT[kL] * inv;
         }
@@ -375,9 +433,9 @@ struct oracle_sim {
       for (int j = ng - 1; j < H - ng; j++) {
         for (int i = ng; i < W - ng; i++) {
           const int kL = j * W + i, kR = kL + W;
-          const double th = fyM[kL] >= 0 ? theta[kL] : theta[kR];
-          const double invL = th / dyRowN[j];
-          const double invR = th / dyRowS[j + 1];
+          const T th = fyM[kL] >= 0 ? theta[kL] : theta[kR];
+          const T invL = th / dyRowN[j];
+          const T invR = th / dyRowS[j + 1];
           rh[kL] -= fyM[kL] * invL; rhv[kL] -= (fyN[kL] + pyL[kL]) * invL; rhu[kL] -= fyT[kL] * invL;
           rh[kR] += fyM[kL] * invR; rhv[kR] += (fyN[kL] + pyR[kL]) * invR; rhu[kR] += fyT[kL] * invR;
         }
@@ -385,33 +443,33 @@ struct oracle_sim {
     } else {
       // The same additions gathered per cell, in the order the scatter loops
       // apply them to that cell: west face, east face, south face, north face.
-#pragma omp parallel for num_threads(T) schedule(static)
+#pragma omp parallel for num_threads(nthr) schedule(static)
       for (int j = 0; j < H; j++) {
         for (int i = 0; i < W; i++) {
           const int k = j * W + i;
-          double a = rh[k], au = rhu[k], av = rhv[k];
+          T a = rh[k], au = rhu[k], av = rhv[k];
           const bool xrow = j >= ng && j < H - ng;
           if (xrow && i - 1 >= ng - 1 && i - 1 < W - ng) {
             const int kL = k - 1;
-            const double th = fxM[kL] >= 0 ? theta[kL] : theta[k];
-            const double inv = th / dxRow[j];
+            const T th = fxM[kL] >= 0 ? theta[kL] : theta[k];
+            const T inv = th / dxRow[j];
             a += fxM[kL] * inv; au += (fxN[kL] + pxR[kL]) * inv; av += fxT[kL] * inv;
           }
           if (xrow && i >= ng - 1 && i < W - ng) {
-            const double th = fxM[k] >= 0 ? theta[k] : theta[k + 1];
-            const double inv = th / dxRow[j];
+            const T th = fxM[k] >= 0 ? theta[k] : theta[k + 1];
+            const T inv = th / dxRow[j];
             a -= fxM[k] * inv; au -= (fxN[k] + pxL[k]) * inv; av -= fxT[k] * inv;
           }
           const bool ycol = i >= ng && i < W - ng;
           if (ycol && j - 1 >= ng - 1 && j - 1 < H - ng) {
             const int kL = k - W;
-            const double th = fyM[kL] >= 0 ? theta[kL] : theta[k];
-            const double invR = th / dyRowS[j];
+            const T th = fyM[kL] >= 0 ? theta[kL] : theta[k];
+            const T invR = th / dyRowS[j];
             a += fyM[kL] * invR; av += (fyN[kL] + pyR[kL]) * invR; au += fyT[kL] * invR;
           }
           if (ycol && j >= ng - 1 && j < H - ng) {
-            const double th = fyM[k] >= 0 ? theta[k] : theta[k + W];
-            const double invL = th / dyRowN[j];
+            const T th = fyM[k] >= 0 ? theta[k] : theta[k + W];
+            const T invL = th / dyRowN[j];
             a -= fyM[k] * invL; av -= (fyN[k] + pyL[k]) * invL; au -= fyT[k] * invL;
           }
           rh[k] = a; rhu[k] = au; rhv[k] = av;
@@ -422,18 +480,18 @@ struct oracle_sim {
     // centred bed term + spherical geometric source, src/swe.mjs:570-598
     if (order >= 2 || sph) {
       const std::vector<double>& geoCoef = g[OG_GEOCOEF];
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
       for (int j = ng; j < H - ng; j++) {
         const double bedDiv1 = bedPhi[j], bedDiv0 = dxRow[j], gc = geoCoef[j];
         for (int i = ng; i < W - ng; i++) {
           const int k = j * W + i, k2 = 2 * k;
-          const double bk = b[k];
-          const double eC = bk + h[k];
+          const T bk = b[k];
+          const T eC = bk + h[k];
           for (int d = 0; d < 2; d++) {
-            const double hP = jmax(0, eC + 0.5 * sE[k2 + d] - (bk + 0.5 * sB[k2 + d]));
-            const double hM = jmax(0, eC - 0.5 * sE[k2 + d] - (bk - 0.5 * sB[k2 + d]));
-            const double db = sB[k2 + d];
-            const double term = -G * 0.5 * (hP + hM) * db / (d == 0 ? bedDiv0 : bedDiv1);
+            const T hP = jmax(0, eC + 0.5 * sE[k2 + d] - (bk + 0.5 * sB[k2 + d]));
+            const T hM = jmax(0, eC - 0.5 * sE[k2 + d] - (bk - 0.5 * sB[k2 + d]));
+            const T db = sB[k2 + d];
+            const T term = -G * 0.5 * (hP + hM) * db / (d == 0 ? bedDiv0 : bedDiv1);
             if (d == 0) rhu[k] += term;
             else {
               rhv[k] += term;
@@ -448,19 +506,19 @@ struct oracle_sim {
     if (sph) {
       const std::vector<double>& fRow = g[OG_FROW];
       const std::vector<double>& tanPhi = g[OG_TANPHI];
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
       for (int j = ng; j < H - ng; j++) {
         const double f0 = fRow[j], tR = tanPhi[j] / R;
         for (int i = ng; i < W - ng; i++) {
           const int k = j * W + i;
-          const double fe = f0 + U[k] * tR;
+          const T fe = f0 + U[k] * tR;
           rhu[k] += fe * hv[k];
           rhv[k] -= fe * hu[k];
         }
       }
     } else if (coriolis != 0 && coriolis == coriolis) {
       const double f = coriolis;
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
       for (int j = ng; j < H - ng; j++) {
         for (int i = ng; i < W - ng; i++) {
           const int k = j * W + i;
@@ -475,39 +533,39 @@ struct oracle_sim {
   double maxDt() const {
     const std::vector<double>& dxRow = g[OG_DXROW];
     const std::vector<double>& dyCFL = g[OG_DYCFL];
-    double inv = 0;
+    T inv = 0;
     for (int j = ng; j < H - ng; j++) {
       for (int i = ng; i < W - ng; i++) {
         const int k = j * W + i;
-        const double hk = h[k];
+        const T hk = h[k];
         if (hk <= minDepth) continue;
-        const double c = std::sqrt(G * hk);
-        const double u = std::fabs(vel(hu[k], hk)), v = std::fabs(vel(hv[k], hk));
-        const double s = (u + c) / dxRow[j] + (v + c) / dyCFL[j];
+        const T c = sqrtT(G * hk);
+        const T u = fabsT(vel(hu[k], hk)), v = fabsT(vel(hv[k], hk));
+        const T s = (u + c) / dxRow[j] + (v + c) / dyCFL[j];
         if (s > inv) inv = s;
       }
     }
-    return inv > 0 ? cfl / inv : INF;
+    return inv > 0 ? cfl / value(inv) : INF;
   }
 
   // src/swe.mjs:659-704
   void applyFriction(double dt) {
     const double n = manning;
-    const int T = threads;
+    const int nthr = threads;
     if (hasManning) {
-      const double* nf = manningField.data();
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+      const T* nf = manningField.data();
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
       for (int j = ng; j < H - ng; j++) {
         for (int i = ng; i < W - ng; i++) {
           const int k = j * W + i;
-          const double hk = h[k];
+          const T hk = h[k];
           if (hk <= minDepth) { hu[k] = 0; hv[k] = 0; continue; }
-          const double nk = nf[k];
+          const T nk = nf[k];
           if (!(nk != 0 && nk == nk)) continue;
-          const double u = vel(hu[k], hk), v = vel(hv[k], hk);
-          const double speed = std::hypot(u, v);
+          const T u = vel(hu[k], hk), v = vel(hv[k], hk);
+          const T speed = hypotT(u, v);
           if (speed < 1e-14) continue;
-          const double denom = 1 + dt * G * nk * nk * speed / std::pow(hk, 4.0 / 3.0);
+          const T denom = 1 + dt * G * nk * nk * speed / powT(hk, 4.0 / 3.0);
           hu[k] /= denom;
           hv[k] /= denom;
         }
@@ -515,16 +573,16 @@ struct oracle_sim {
       return;
     }
     if (!(n != 0 && n == n)) return;
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
     for (int j = ng; j < H - ng; j++) {
       for (int i = ng; i < W - ng; i++) {
         const int k = j * W + i;
-        const double hk = h[k];
+        const T hk = h[k];
         if (hk <= minDepth) { hu[k] = 0; hv[k] = 0; continue; }
-        const double u = vel(hu[k], hk), v = vel(hv[k], hk);
-        const double speed = std::hypot(u, v);
+        const T u = vel(hu[k], hk), v = vel(hv[k], hk);
+        const T speed = hypotT(u, v);
         if (speed < 1e-14) continue;
-        const double denom = 1 + dt * G * n * n * speed / std::pow(hk, 4.0 / 3.0);
+        const T denom = 1 + dt * G * n * n * speed / powT(hk, 4.0 / 3.0);
         hu[k] /= denom;
         hv[k] /= denom;
       }
@@ -532,8 +590,8 @@ struct oracle_sim {
   }
 
   // src/swe.mjs:734-745
-  double dryClean() {
-    double added = 0;
+  T dryClean() {
+    T added = 0;
     for (int j = ng; j < H - ng; j++) {
       for (int i = ng; i < W - ng; i++) {
         const int k = j * W + i;
@@ -549,8 +607,8 @@ struct oracle_sim {
     const double ref = spongeRef;
     for (const auto& c : spongeCells) {
       const int k = c.first;
-      const double f = jmin(1, c.second * dt * 60);
-      const double target = jmax(0, ref - b[k]);
+      const double f = jmin(1.0, c.second * dt * 60);
+      const T target = jmax(0, ref - b[k]);
       h[k] += (target - h[k]) * f;
       hu[k] -= hu[k] * f;
       hv[k] -= hv[k] * f;
@@ -563,9 +621,9 @@ struct oracle_sim {
     const double hh = self ? maxDt() : dtIn;
     if (!(hh > 0) || !std::isfinite(hh)) return 0;
     h0 = h; hu0 = hu; hv0 = hv;
-    const int T = threads;
+    const int nthr = threads;
     residual(hh);
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
     for (int k = 0; k < N; k++) {
       h[k] += hh * rh[k];
       hu[k] += hh * rhu[k];
@@ -574,7 +632,7 @@ struct oracle_sim {
     massFloored = dryClean();
     applyBC();
     residual(hh);
-#pragma omp parallel for num_threads(T) if (T > 1) schedule(static)
+#pragma omp parallel for num_threads(nthr) if (nthr > 1) schedule(static)
     for (int k = 0; k < N; k++) {
       h[k] = 0.5 * (h0[k] + h[k] + hh * rh[k]);
       hu[k] = 0.5 * (hu0[k] + hu[k] + hh * rhu[k]);
@@ -589,32 +647,32 @@ struct oracle_sim {
   }
 
   // src/swe.mjs:819-836
-  double volume() const {
+  T volume() const {
     if (!sphere) {
-      double v = 0;
+      T v = 0;
       for (int j = 0; j < ny; j++) for (int i = 0; i < nx; i++) v += h[(j + ng) * W + (i + ng)];
       return v * dx * dy;
     }
     const std::vector<double>& area = g[OG_AREA];
-    double v = 0;
+    T v = 0;
     for (int j = 0; j < ny; j++) {
-      double row = 0;
+      T row = 0;
       for (int i = 0; i < nx; i++) row += h[(j + ng) * W + (i + ng)];
       v += row * area[j + ng];
     }
     return v;
   }
   // src/swe.mjs:862-877
-  double energy() const {
+  T energy() const {
     const std::vector<double>& area = g[OG_AREA];
-    double e = 0;
+    T e = 0;
     for (int j = 0; j < ny; j++) {
-      double row = 0;
+      T row = 0;
       for (int i = 0; i < nx; i++) {
         const int k = (j + ng) * W + (i + ng);
-        const double hk = h[k];
+        const T hk = h[k];
         if (hk <= 0) continue;
-        const double u = vel(hu[k], hk), v = vel(hv[k], hk);
+        const T u = vel(hu[k], hk), v = vel(hv[k], hk);
         row += 0.5 * hk * (u * u + v * v) + 0.5 * G * hk * (hk + 2 * b[k]);
       }
       if (sphere) e += row * area[j + ng]; else e += row;
@@ -622,26 +680,26 @@ struct oracle_sim {
     return sphere ? e : e * dx * dy;
   }
   // src/swe.mjs:880-892
-  double maxSurfaceDeviation(double ref) const {
-    double m = 0;
+  T maxSurfaceDeviation(double ref) const {
+    T m = 0;
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++) {
         const int k = (j + ng) * W + (i + ng);
         if (h[k] <= minDepth) continue;
-        const double d = std::fabs(b[k] + h[k] - ref);
+        const T d = fabsT(b[k] + h[k] - ref);
         if (d > m) m = d;
       }
     return m;
   }
   // src/swe.mjs:895-907
-  double maxSpeed() const {
-    double m = 0;
+  T maxSpeed() const {
+    T m = 0;
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++) {
         const int k = (j + ng) * W + (i + ng);
-        const double hk = h[k];
+        const T hk = h[k];
         if (hk <= minDepth) continue;
-        const double s = std::hypot(vel(hu[k], hk), vel(hv[k], hk));
+        const T s = hypotT(vel(hu[k], hk), vel(hv[k], hk));
         if (s > m) m = s;
       }
     return m;
@@ -649,13 +707,16 @@ struct oracle_sim {
   // src/swe.mjs:912-917
   bool finite() const {
     for (int k = 0; k < N; k++)
-      if (!std::isfinite(h[k]) || !std::isfinite(hu[k]) || !std::isfinite(hv[k])) return false;
+      if (!isfiniteT(h[k]) || !isfiniteT(hu[k]) || !isfiniteT(hv[k])) return false;
     return true;
   }
 };
 
+struct oracle_sim : SimT<double> {};
+
 // ---- metric, src/geometry.mjs ------------------------------------------------
-static void cartesianGeometry(oracle_sim* s) {     // src/geometry.mjs:163-176
+template <class S>
+static void cartesianGeometry(S* s) {               // src/geometry.mjs:163-176
   s->R = INF;
   s->dlam = 0; s->dphi = 0;
   s->totalArea = s->nx * s->dx * s->ny * s->dy;
@@ -869,5 +930,54 @@ int    oracle_finite(oracle_sim* s) { return s->finite() ? 1 : 0; }
 double oracle_vel(oracle_sim* s, double hq, double h) { return s->vel(hq, h); }
 void   oracle_hllc(double* out3, double hL, double huL, double hvL, double hR, double huR,
                    double hvR, double dry) { hllc(out3, hL, huL, hvL, hR, huR, hvR, dry); }
+
+// Tangent-linear model of the gauge misfit J = sum_steps sum_gauges
+// (b + h - obs)^2 over `steps` self-timed steps from h = max(0, eta0 - b)
+// (Cartesian, walls): the solver run on Duals seeded with the directions db
+// (bed) and dn (Manning field; NULL n means the scalar o->manning).  dt is
+// each step's maxDt() of the value part, held as a constant, as the adjoint
+// holds it.  Returns J, dJ = <grad J, (db, dn)>, and the dt sequence.
+int oracle_tlm_misfit(const oracle_options* o, const double* b, const double* eta0, const double* n,
+                      const double* db, const double* dn, int ng, const int* gauges, int steps,
+                      const double* obs, int threads, double* J, double* dJ, double* dts) {
+  if (!o || o->sphere || !b || !eta0 || !db || ng < 1 || !gauges || steps < 1 || !obs) {
+    g_err = "oracle_tlm_misfit: Cartesian options, b, eta0, db, gauges, steps, obs"; return -1;
+  }
+  SimT<Dual> s;
+  s.nx = o->nx; s.ny = o->ny; s.ng = 2; s.W = s.nx + 4; s.H = s.ny + 4; s.N = s.W * s.H;
+  s.dx = o->dx; s.dy = o->dy; s.manning = o->manning; s.minDepth = o->min_depth; s.cfl = o->cfl;
+  s.coriolis = o->coriolis; s.eps4 = std::pow(jmax(o->min_depth, 1e-12), 4.0);
+  s.order = o->order; s.limiter = o->limiter; s.sphere = 0; s.threads = threads < 1 ? 1 : threads;
+  for (int r = 0; r < OG_NROWS; r++) s.g[r].assign(s.H, 0.0);
+  cartesianGeometry(&s);
+  const int N = s.N;
+  for (auto* v : {&s.b, &s.h, &s.hu, &s.hv, &s.h0, &s.hu0, &s.hv0, &s.rh, &s.rhu, &s.rhv, &s.fxM, &s.fxN,
+                  &s.fxT, &s.fyM, &s.fyN, &s.fyT, &s.pxL, &s.pxR, &s.pyL, &s.pyR, &s.theta, &s.uu, &s.vv})
+    v->assign(N, Dual(0));
+  for (auto* v : {&s.sE, &s.sU, &s.sV, &s.sB}) v->assign(2 * N, Dual(0));
+  for (int k = 0; k < N; k++) {
+    s.b[k] = Dual(b[k], db[k]);
+    s.h[k] = jmax(Dual(0), Dual(eta0[k]) - s.b[k]);
+  }
+  if (n) {
+    s.manningField.resize(N);
+    for (int k = 0; k < N; k++) s.manningField[k] = Dual(n[k], dn ? dn[k] : 0);
+    s.hasManning = true;
+  }
+  Dual acc(0);
+  for (int st = 0; st < steps; st++) {
+    s.applyBC();
+    const double dt = s.maxDt();
+    if (dts) dts[st] = dt;
+    s.step(dt, false);
+    for (int q = 0; q < ng; q++) {
+      const Dual r = s.b[gauges[q]] + s.h[gauges[q]] - obs[(size_t)st * ng + q];
+      acc += r * r;
+    }
+  }
+  *J = acc.v;
+  *dJ = acc.d;
+  return 0;
+}
 
 }  // extern "C"

@@ -82,6 +82,11 @@ double       oracle_vel(oracle_sim* s, double hq, double h);
 void         oracle_hllc(double* out3, double hL, double huL, double hvL, double hR, double huR,
                          double hvR, double dry);
 
+/* Tangent-linear model of the gauge misfit (see swe_oracle.cpp). */
+int          oracle_tlm_misfit(const oracle_options* o, const double* b, const double* eta0, const double* n,
+                               const double* db, const double* dn, int ng, const int* gauges, int steps,
+                               const double* obs, int threads, double* J, double* dJ, double* dts);
+
 #ifdef __cplusplus
 }
 #endif

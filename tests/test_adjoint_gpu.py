@@ -1,0 +1,87 @@
+"""The discrete adjoint on the GPU: its gradient against the tangent-linear
+reference (the oracle on dual numbers, same frozen dt sequence) and against
+central differences of the GPU forward, for random directions in the bed and
+the Manning field; and the same gradient whatever the checkpoint interval."""
+import numpy as np
+import pytest
+
+from tlm import tlm_misfit
+
+pytestmark = pytest.mark.gpu
+
+
+def case(swe, nx=40, ny=30, steps=30, seed=21):
+    from water_simulator_b200 import workloads
+    c = workloads.adjoint_case(nx=nx, ny=ny, dx=10.0, n_gauges=6, seed=seed, hump=0.4)
+    # observations from the perturbed bed
+    truth = swe.MisfitAdjoint(nx, ny, 10.0, c["b_true"], c["eta0"], manning_field=c["n"], gauges=c["gauges"],
+                              steps=steps, checkpoint_every=7)
+    _, eta = truth.forward()
+    truth.close()
+    return c, eta
+
+
+def gradient(swe, c, obs, steps, every=7):
+    adj = swe.MisfitAdjoint(c["nx"], c["ny"], c["dx"], c["b"], c["eta0"], manning_field=c["n"], gauges=c["gauges"],
+                            steps=steps, checkpoint_every=every)
+    adj.set_observations(obs)
+    J, _ = adj.forward()
+    gb, gn = adj.backward()
+    dts = adj.dt_sequence()
+    return adj, J, gb, gn, dts
+
+
+def test_adjoint_matches_tangent_linear(swe):
+    steps = 30
+    c, obs = case(swe, steps=steps)
+    adj, J, gb, gn, dts = gradient(swe, c, obs, steps)
+    rng = np.random.default_rng(1)
+    for trial in range(4):
+        db = rng.normal(0, 1, c["b"].shape)
+        dn = rng.normal(0, 1e-3, c["n"].shape) if trial >= 2 else np.zeros(c["n"].shape)
+        Jt, dJ, dts_t = tlm_misfit(c, c["b"], c["n"], db, dn, steps, obs)
+        assert abs(Jt - J) <= 1e-12 * abs(J)
+        got = float(np.dot(gb, db.reshape(-1)) + np.dot(gn, dn.reshape(-1)))
+        assert abs(got - dJ) <= 1e-8 * abs(dJ), (trial, got, dJ)
+    assert np.all(gb.reshape(c["ny"] + 4, c["nx"] + 4)[:2] == 0)          # ghosts carry no gradient
+    adj.close()
+
+
+def test_adjoint_against_central_differences(swe):
+    steps = 30
+    c, obs = case(swe, steps=steps, seed=22)
+    adj, J, gb, gn, dts = gradient(swe, c, obs, steps)
+    rng = np.random.default_rng(2)
+
+    def J_at(b, n):
+        f = swe.MisfitAdjoint(c["nx"], c["ny"], c["dx"], b, c["eta0"], manning_field=n, gauges=c["gauges"],
+                              steps=steps, checkpoint_every=steps)
+        f.set_observations(obs)
+        f.dt_sequence(fixed=dts)
+        v, _ = f.forward()
+        f.close()
+        return v
+
+    for trial in range(20):
+        db = rng.normal(0, 1, c["b"].shape)
+        dn = rng.normal(0, 1e-3, c["n"].shape)
+        want = float(np.dot(gb, db.reshape(-1)) + np.dot(gn, dn.reshape(-1)))
+        errs = []
+        for eps in (1e-4, 1e-5, 1e-6, 1e-7):
+            fd = (J_at(c["b"] + eps * db, c["n"] + eps * dn) - J_at(c["b"] - eps * db, c["n"] - eps * dn)) / (2 * eps)
+            errs.append(abs(fd - want) / abs(want))
+        assert min(errs) <= 1e-5, (trial, errs)
+    adj.close()
+
+
+def test_gradient_independent_of_checkpointing(swe):
+    steps = 23
+    c, obs = case(swe, steps=steps, seed=23)
+    ref = None
+    for every in (1, 5, 23):
+        adj, J, gb, gn, _ = gradient(swe, c, obs, steps, every)
+        if ref is None:
+            ref = (gb, gn)
+        else:
+            assert np.array_equal(gb, ref[0]) and np.array_equal(gn, ref[1])
+        adj.close()

@@ -1,0 +1,45 @@
+"""Test helpers for the misfit's tangent-linear reference (the oracle run on
+dual numbers, oracle_tlm_misfit) and for finite differences on the oracle."""
+import ctypes
+
+import numpy as np
+
+from oracle_sim import OracleOptions, OracleSim, oracle_lib, _dp
+
+
+def tlm_misfit(case, b, n, db, dn, steps, obs, threads=1):
+    lib = oracle_lib()
+    fn = lib.oracle_tlm_misfit
+    D, I, DP = ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
+    fn.argtypes = [ctypes.POINTER(OracleOptions), DP, DP, DP, DP, DP, I, ctypes.POINTER(ctypes.c_int), I, DP, I,
+                   ctypes.POINTER(D), ctypes.POINTER(D), DP]
+    fn.restype = I
+    o = OracleOptions()
+    o.nx, o.ny, o.dx, o.dy = case["nx"], case["ny"], case["dx"], case["dx"]
+    o.manning, o.min_depth, o.cfl, o.coriolis, o.order, o.limiter, o.sphere = 0.025, 1e-3, 0.45, 0.0, 2, 0, 0
+    g = np.ascontiguousarray(case["gauges"], dtype=np.int32)
+    arrs = [np.ascontiguousarray(x, dtype=np.float64).reshape(-1) for x in (b, case["eta0"], n, db, dn)]
+    ob = np.ascontiguousarray(obs, dtype=np.float64).reshape(-1)
+    J, dJ = D(), D()
+    dts = np.zeros(steps)
+    rc = fn(ctypes.byref(o), _dp(arrs[0]), _dp(arrs[1]), _dp(arrs[2]), _dp(arrs[3]), _dp(arrs[4]), len(g),
+            g.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), steps, _dp(ob), threads, ctypes.byref(J),
+            ctypes.byref(dJ), _dp(dts))
+    assert rc == 0, lib.oracle_last_error()
+    return J.value, dJ.value, dts
+
+
+def oracle_misfit(case, b, n, steps, obs, dts):
+    """J on the oracle (doubles) with the dt sequence held fixed."""
+    sim = OracleSim(nx=case["nx"], ny=case["ny"], dx=case["dx"], bed=np.asarray(b), eta0=case["eta0"], manning=0.025)
+    sim.setManningField(n)
+    J = 0.0
+    g = case["gauges"]
+    for s in range(steps):
+        sim.step(float(dts[s]))
+        hb = sim.b[g] + sim.h[g]
+        for q in range(len(g)):
+            r = hb[q] - obs[s][q]
+            J += r * r
+    sim.close()
+    return J

@@ -13,9 +13,10 @@ from .swe import (G, R_EARTH, OMEGA_EARTH, ShallowWater, Flather, Sponge, hllc, 
 from .tide import Tide, TideSignal, CONSTITUENTS, ATLANTIC_MESO, DIURNAL_COAST
 from ._lib import SweError, load as load_library, LIB_PATH
 from .batch import Ensemble
+from .adjoint import MisfitAdjoint
 
 __all__ = ["G", "R_EARTH", "OMEGA_EARTH", "ShallowWater", "Flather", "Sponge", "hllc", "hllc_batch",
            "reflect", "outflow", "periodic", "flather", "makeSponge", "cartesianGeometry",
            "sphericalGeometry", "interiorArea", "cellLonLat", "Geometry", "Tide", "TideSignal",
            "CONSTITUENTS", "ATLANTIC_MESO", "DIURNAL_COAST", "SweError", "load_library", "LIB_PATH",
-           "Ensemble"]
+           "Ensemble", "MisfitAdjoint"]

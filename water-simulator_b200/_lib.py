@@ -102,6 +102,13 @@ SIGNATURES = {
     "swe_batch_get_stream": [_P, ctypes.POINTER(_P)],
     "swe_batch_get_field": [_P, _I, _I, _DP],
     "swe_batch_get_scalar": [_P, _I, _I, _DP],
+    "swe_adjoint_create": [ctypes.POINTER(SweOptions), _DP, _DP, _DP, _I, _IP, _I, _I, ctypes.POINTER(_P)],
+    "swe_adjoint_destroy": [_P],
+    "swe_adjoint_set_observations": [_P, _DP],
+    "swe_adjoint_forward": [_P, _DP, _DP],
+    "swe_adjoint_backward": [_P, _DP, _DP],
+    "swe_adjoint_dt_sequence": [_P, _DP, _DP],
+    "swe_adjoint_get_stream": [_P, ctypes.POINTER(_P)],
 }
 _RESTYPES = {"swe_last_error": ctypes.c_char_p}
 

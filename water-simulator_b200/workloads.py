@@ -100,3 +100,29 @@ def ensemble(n=256, seed=4, dx=5.0, amp=0.5, eta=2.0):
                     "tide": {"msl": eta, "amp": [amp], "omega": [2 * math.pi / (period_h * 3600)],
                              "phase_deg": [0.0]}})
     return out
+
+
+def adjoint_case(nx=1024, ny=1024, dx=10.0, n_gauges=32, seed=5, hump=0.5, noise=0.1, manning_lo=0.015,
+                 manning_hi=0.04):
+    """The adjoint workload: a bump-and-roughness bed (bump 1.5 m high,
+    sigma 40 cells, roughness +/- 0.2 m) under still water at 2 m with a
+    released Gaussian hump of `hump` m (sigma 25 cells) to set it moving;
+    a per-cell Manning field ~ U[0.015, 0.04]; n_gauges seeded interior
+    gauge cells; and the 'true' bed b + N(0, noise) that makes the synthetic
+    observations.  Returns a dict with padded arrays b, b_true, eta0, n and
+    the gauge indices k = j*W + i."""
+    rng = np.random.default_rng(seed)
+    W, H = nx + 4, ny + 4
+    X, Y = _centres(nx, ny, dx)
+    cx, cy = nx * dx / 2, ny * dx / 2
+    s = 40 * dx
+    b = 1.5 * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * s * s)) + uniform_noise(seed, X.shape, -0.2, 0.2)
+    sh = 25 * dx
+    hx, hy = 0.3 * nx * dx, 0.6 * ny * dx
+    eta0 = 2.0 + hump * np.exp(-((X - hx) ** 2 + (Y - hy) ** 2) / (2 * sh * sh))
+    n = rng.uniform(manning_lo, manning_hi, X.shape)
+    gi = rng.integers(2, nx + 2, n_gauges)
+    gj = rng.integers(2, ny + 2, n_gauges)
+    gauges = (gj * W + gi).astype(np.int32)
+    b_true = b + rng.normal(0.0, noise, X.shape)
+    return {"nx": nx, "ny": ny, "dx": dx, "b": b, "b_true": b_true, "eta0": eta0, "n": n, "gauges": gauges}
