@@ -29,6 +29,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -48,8 +50,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="beach", choices=["beach", "ensemble"],
-                   help="beach: the 2048x2048 headline; ensemble: the 256-basin batched form vs the plain kernel")
+    p.add_argument("--workload", default="beach", choices=["beach", "ensemble", "adjoint", "sphere"],
+                   help="beach: the 2048x2048 headline; ensemble: the 256-basin batched form vs the plain "
+                        "kernel; sphere: the 1440x720 tide; adjoint: the 1024x1024 misfit gradient")
+    p.add_argument("--stage", default="default", choices=["default", "fused", "split"],
+                   help="stage kernels: the library default, the fused row-marching kernel or the tiled pair")
     p.add_argument("--nx", type=int, default=2048, help="grid size (the workload is 2048x2048)")
     p.add_argument("--ny", type=int, default=2048)
     a = p.parse_args()
@@ -422,12 +427,196 @@ def run_ensemble(args):
     return 0
 
 
+SPHERE_OMEGA = 7.2921e-5
+M2_HOURS = 12.42
+
+
+def run_sphere(args):
+    """The 1440 x 720 spherical tide workload (0.25 degrees in longitude,
+    band 85S..85N), longitude periodic, Flather M2 tide (1 m, 12.42 h) on
+    the south and north cap edges, Coriolis on (Earth's rotation), wetting
+    and drying over 30% land, dt = maxDt() each step; 5000 steps through the
+    device loop.
+    The first steps are checked bit for bit against the oracle on the same
+    input, and the oracle gives the CPU baseline on a bounded sample."""
+    import torch
+    import __graft_entry__
+    swe = __graft_entry__.load_package()
+    from water_simulator_b200 import workloads
+    c = workloads.globe_tide()
+    nx, ny = c["nx"], c["ny"]
+    sphere = {"R": 6371e3, "lat0": c["lat0"], "lat1": c["lat1"], "omega": SPHERE_OMEGA}
+    tide = swe.Tide({"M2": [1.0, 0.0]}, periods_hours={"M2": M2_HOURS})
+    K = int(os.environ.get("SWE_SPHERE_STEPS", "5000"))
+
+    def make():
+        sim = swe.ShallowWater(nx=nx, ny=ny, bed=c["b"], eta0=c["eta0"], sphere=sphere)
+        sim.boundaries = {"south": swe.flather(tide.signal()), "north": swe.flather(tide.signal())}
+        return sim
+
+    def oracle(threads):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_sim import OracleSim
+        o = OracleSim(nx=nx, ny=ny, bed=c["b"], eta0=c["eta0"], sphere=sphere, threads=threads)
+        tr = tide.terms
+        row = ("tide", tide.msl, [k["amp"] for k in tr], [k["omega"] for k in tr], [k["phase"] for k in tr], 0.0)
+        o.set_boundaries(west="periodic", east="periodic", south=row, north=row)
+        return o
+
+    # parity of the first steps at full size (bit-exact fields, same t)
+    chk = 3
+    sim = make()
+    sim.run(chk)
+    ref = oracle(os.cpu_count() or 1)
+    for _ in range(chk):
+        ref.step()
+    exact = all(np.array_equal(sim.field(f), ref.field(f)) for f in ("h", "hu", "hv")) and sim.t == ref.t
+    rel = max(float(np.max(np.abs(sim.field(f) - ref.field(f))) / max(np.max(np.abs(ref.field(f))), 1e-300))
+              for f in ("h", "hu", "hv"))
+    ref.close()
+    sim.close()
+
+    sim = make()
+    sp = ctypes.c_void_p()
+    lib = swe.load_library()
+    swe._lib.check(lib.swe_get_stream(sim._h, ctypes.byref(sp)))
+    st = torch.cuda.ExternalStream(sp.value)
+    sim.run(max(args.warmup, 3))
+    sim.synchronize()
+    sampler = ClockSampler(0)
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    done = sim.run(K)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    if done != K:
+        raise RuntimeError(f"the device loop took {done} of {K} steps")
+    value = nx * ny * K / (ms / 1e3)
+    dt_last = sim.maxDt()
+    finite = sim.finite()
+    sim.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        o = oracle(1)
+        o.step()
+        n, t0 = 0, time.perf_counter()
+        while True:
+            o.step()
+            n += 1
+            el = time.perf_counter() - t0
+            if el >= 12.0 or n >= 40:
+                break
+        o.close()
+        cpu = {"value": nx * ny * n / el, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{n} self-timed steps of the same sphere workload ({el:.1f} s) on the oracle, 1 thread"}
+    line = {"metric": "FP64 cell-updates/s, sphere", "value": value, "unit": UNIT, "n_gpus": 1, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"sphere {nx}x{ny}, 0.25 deg longitude, lat {c['lat0']}..{c['lat1']} "
+                                   "(the whole sphere has no open edge), band-limited bed 0-5000 m deep with the "
+                                   "30% highest cells land at +50 m, still water, Flather M2 tide 1 m (12.42 h) on "
+                                   "the S and N cap edges, Coriolis omega 7.2921e-5, Manning 0.025, dt = maxDt()",
+                       "cells": nx * ny, "l2": "state 3 x 8.4 MB per copy: fits L2; steady-state stream"},
+            "first_steps_vs_oracle": {"steps": chk, "bit_exact": exact, "max_rel_err": rel}, "finite": finite, "dt_last": dt_last,
+            "gpu_launches": 5 * K, "clocks": clocks, "cpu_baseline": cpu}
+    print(json.dumps(line))
+    return 0
+
+
+def run_adjoint(args):
+    """Gradient of the gauge misfit on the 1024 x 1024 case: the cost of one
+    gradient (forward with checkpoints + backward) against the plain forward
+    of the same steps, and a central-difference check on random directions."""
+    import torch
+    import __graft_entry__
+    swe = __graft_entry__.load_package()
+    from water_simulator_b200 import workloads
+    n = int(os.environ.get("SWE_ADJ_N", "1024"))
+    steps = int(os.environ.get("SWE_ADJ_STEPS", "2000"))
+    ndir = int(os.environ.get("SWE_ADJ_DIRS", "20"))
+    c = workloads.adjoint_case(nx=n, ny=n, dx=10.0, n_gauges=32)
+    kw = dict(manning_field=c["n"], gauges=c["gauges"], steps=steps, checkpoint_every=45)
+    truth = swe.MisfitAdjoint(n, n, 10.0, c["b_true"], c["eta0"], **kw)
+    _, obs = truth.forward()
+    truth.close()
+    def timed(stream_ptr, fn):
+        st = torch.cuda.ExternalStream(stream_ptr)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        out = fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3
+
+    def stream_of(sim):
+        sp = ctypes.c_void_p()
+        swe._lib.check(swe._lib.load().swe_get_stream(sim._h, ctypes.byref(sp)))
+        return sp.value
+
+    # plain forward: the same self-timed steps through the device loop (warm one run first)
+    t_plain = None
+    for _ in range(2):
+        sim = swe.ShallowWater(nx=n, ny=n, dx=10.0, bed=c["b"], eta0=c["eta0"])
+        sim.setManningField(c["n"])
+        sim.synchronize()
+        _, t_plain = timed(stream_of(sim), lambda: sim.run(steps))
+        sim.close()
+    adj = swe.MisfitAdjoint(n, n, 10.0, c["b"], c["eta0"], **kw)
+    adj.set_observations(obs)
+    (J, _), t_fwd = timed(adj.stream(), adj.forward)
+    (gb, gn), t_bwd = timed(adj.stream(), adj.backward)
+    dts = adj.dt_sequence()
+    rng = np.random.default_rng(7)
+    errs = []
+    for _ in range(ndir):
+        db = rng.normal(0, 1, c["b"].shape)
+        dn = rng.normal(0, 1e-3, c["n"].shape)
+        want = float(np.dot(gb, db.reshape(-1)) + np.dot(gn, dn.reshape(-1)))
+        best = math.inf
+        for eps in (1e-6, 1e-5, 1e-7):
+            vals = []
+            for sgn in (1, -1):
+                f = swe.MisfitAdjoint(n, n, 10.0, c["b"] + sgn * eps * db, c["eta0"],
+                                      **dict(kw, manning_field=c["n"] + sgn * eps * dn, checkpoint_every=steps))
+                f.set_observations(obs)
+                f.dt_sequence(fixed=dts)
+                vals.append(f.forward()[0])
+                f.close()
+            best = min(best, abs((vals[0] - vals[1]) / (2 * eps) - want) / abs(want))
+            if best <= 1e-5:
+                break
+        errs.append(best)
+    adj.close()
+    line = {"metric": "adjoint gradient / forward time ratio", "value": (t_fwd + t_bwd) / t_plain,
+            "unit": "x forward", "higher_is_better": False, "n_gpus": 1, "steps": steps, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"{n}x{n} dx=10 m, bump+roughness bed, 0.5 m released hump over 2 m still water, "
+                                   "Manning field U[0.015,0.04], 32 gauges, observations from bed + N(0,0.1) noise, "
+                                   "checkpoint every 45 steps", "cells": n * n},
+            "forward_plain_s": t_plain, "forward_recording_s": t_fwd, "backward_s": t_bwd,
+            "backward_over_forward": t_bwd / t_plain, "J": J,
+            "fd_check": {"directions": ndir, "max_rel_err": max(errs) if errs else None,
+                         "median_rel_err": float(np.median(errs)) if errs else None}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
+    if args.stage != "default":
+        os.environ["SWE_B200_STAGE"] = args.stage
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "ensemble":
         return run_ensemble(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
+    if args.workload == "sphere":
+        return run_sphere(args)
     return run_ours(args)
 
 

@@ -270,6 +270,97 @@ int swe_adjoint_get_stream(swe_adjoint* s, void** stream);
  * ny is limited to SWE_NOALLOC_MAX_ROWS (larger grids get SWE_EINVAL), calls
  * that overlap on the GPU race, and the first call on each device looks the
  * array up and should come before any stream capture. */
+/* ---- stage kernels -----------------------------------------------------------
+ * Two implementations of each SSP-RK2 stage, bit-identical in their results:
+ * SWE_STAGE_FUSED, one row-marching kernel per stage that keeps the stencil
+ * on chip; SWE_STAGE_SPLIT, two tiled kernels (faces, then cells) that run
+ * at higher occupancy through 14 extra fields in device memory (the
+ * default).  The environment variable SWE_B200_STAGE=fused|split overrides
+ * the default at creation. */
+#define SWE_STAGE_FUSED 0
+#define SWE_STAGE_SPLIT 1
+int swe_set_stage_kernels(swe_sim* s, int impl);
+int swe_get_stage_kernels(swe_sim* s, int* impl);
+
+/* ---- gridlands terrain import (src/gridlands.mjs) -------------------------
+ * A gridlands-terrain v1 export carries width x height float32 layers
+ * (bedM, surfaceM, optional manningN), little-endian, base64-encoded, row 0 =
+ * north.  The JSON document is parsed by the caller (gridlandsTerrain() checks
+ * format, version, grid and rowOrder); the layers go to the device as text and
+ * are decoded there.  Sampling follows gridlandsTerrain(): bed bilinear in
+ * the export's cells, clamped at the edges (so the two ghost rings get
+ * constant extrapolation), surface and Manning nearest-cell, with the row flip
+ * that makes the sim's +y north (src/gridlands.mjs:262-291); the per-cell
+ * Manning sampler is the one tools/verify-gridlands.mjs:330-331 hands to
+ * setManningField(). */
+typedef struct swe_gridlands {
+  int width, height;           /* grid.width, grid.height: the export's cells */
+  double cell_m;               /* grid.cellMeters */
+  int flip_rows;               /* 1 (the default): export row 0 is the sim's top (north) row */
+  const char* bed_b64;      size_t bed_len;       /* layers.bedM.data */
+  const char* surface_b64;  size_t surface_len;   /* layers.surfaceM.data */
+  const char* manning_b64;  size_t manning_len;   /* layers.manningN.data, or NULL */
+  /* Host float32 layers used instead of the text when non-NULL (e.g. after
+   * settleLakes() has lowered perched lakes on the host). */
+  const float* bed_f32; const float* surface_f32; const float* manning_f32;
+  int manning_field;           /* 1: also set the per-cell Manning field */
+} swe_gridlands;
+
+/* decodeF32 (src/gridlands.mjs:82-98) on the device: `len` characters of
+ * base64 (standard or URL-safe alphabet, '=' padding optional) must decode to
+ * exactly 4*n bytes, else SWE_EINVAL with the reference's message; writes n
+ * floats to the host array `out`. */
+int swe_gridlands_decode(const char* b64, size_t len, int n, float* out);
+
+/* new ShallowWater({nx, ny, dx, dy, bed: t.bed, eta0: t.eta0, ...}) over an
+ * imported terrain: o gives the grid (normally nx = width, ny = height,
+ * dx = dy = cell_m; a finer or coarser grid samples the same functions) and
+ * the solver options.  Cartesian only (SWE_EINVAL for a sphere).  With
+ * manning_field set, a negative or non-finite n is refused as
+ * setManningField() refuses it. */
+int swe_gridlands_create(const swe_options* o, const swe_gridlands* g, swe_sim** out);
+
+/* ---- headless frames (src/render.mjs, src/globe.mjs) ------------------------
+ * RGBA bytes written into a device buffer (rgba_device, when non-NULL) and/or
+ * copied to the host (rgba_host), stored as the reference's ImageData stores
+ * a double (clamped to [0, 255], round half to even, NaN as 0).  No graphics
+ * API is involved. */
+
+/* The map panel of WaterView.draw() (src/render.mjs:220-247): nx * ny pixels,
+ * row 0 = the sim's top row (+y up); water by the diverging ramp about `msl`
+ * at full colour `scale` metres, darkened by the still depth when show_bed;
+ * dry cells by the land ramp. */
+int swe_render_map(swe_sim* s, double msl, double scale, int show_bed, unsigned char* rgba_host, void* rgba_device);
+
+/* The colour tables, for checking: RAMP of src/render.mjs:118-131 (3 * 1025
+ * doubles, unclamped sRGB) and CBYTES of src/globe.mjs:644-652 (3 * 1025
+ * bytes).  Either pointer may be NULL. */
+int swe_render_tables(double* ramp, unsigned char* cbytes);
+
+/* buildGlobeLut(cam, gridOf(sim), style) (src/globe.mjs:554-629): the
+ * pixel -> cell table of a size x size orthographic view at `tilt_deg`
+ * with the disc inscribed at `margin`, baked once on the host and kept on
+ * the device.  sun, bg, halo: 3 values each or NULL for the reference's
+ * defaults ([-0.42, 0.48, 0.77], [8, 11, 16], [36, 58, 84]).  Spherical
+ * sims only (SWE_EINVAL otherwise, as gridOf() throws). */
+typedef struct swe_globe_lut swe_globe_lut;
+int swe_globe_lut_create(swe_sim* s, int size, double tilt_deg, double margin, const double* sun,
+                         const double* bg, const double* halo, swe_globe_lut** out);
+int swe_globe_lut_destroy(swe_globe_lut* lut);
+/* counts[4] = count (modelled pixels), inside (pixels on the disc), capped
+ * (disc pixels outside the modelled band), size; then the table itself
+ * (count entries each: byte offset, longitude at rotation 0 [deg], padded
+ * index of the row's first interior cell, float32 light) and the baked
+ * background (4 * size * size bytes).  Any pointer may be NULL. */
+int swe_globe_lut_get(swe_globe_lut* lut, int* counts, int* px, double* lon_base, int* row_base, float* lit,
+                      unsigned char* bg);
+/* renderGlobe(out, sim, {lut, rotDeg, scale, msl, landLight})
+ * (src/globe.mjs:770-812).  stats[8] = wet, dry, capped, inside, etaMin,
+ * etaMax, sat, satFrac (may be NULL).  SWE_EINVAL when the grid is not the
+ * one the table was baked for. */
+int swe_render_globe(swe_sim* s, swe_globe_lut* lut, double rot_deg, double scale, double msl, int land_light,
+                     unsigned char* rgba_host, void* rgba_device, double* stats);
+
 #define SWE_NOALLOC_MAX_ROWS 16384
 int swe_max_dt_noalloc(int nx, int ny, const double* h, const double* hu, const double* hv,
                        const double* dx_row, const double* dy_cfl, double min_depth, double cfl,

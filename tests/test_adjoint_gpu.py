@@ -85,3 +85,21 @@ def test_gradient_independent_of_checkpointing(swe):
         else:
             assert np.array_equal(gb, ref[0]) and np.array_equal(gn, ref[1])
         adj.close()
+
+
+def test_gauges_sharing_a_cell(swe):
+    """Gauges may repeat a cell: their contributions add in gauge order."""
+    steps = 20
+    c, _ = case(swe, steps=steps, seed=24)
+    g = np.asarray(c["gauges"], dtype=np.int32)
+    c["gauges"] = np.concatenate([g, g[:2], g[:1]]).astype(np.int32)
+    rng = np.random.default_rng(3)
+    obs = rng.normal(2.0, 0.05, (steps, len(c["gauges"])))
+    adj, J, gb, gn, dts = gradient(swe, c, obs, steps)
+    db = rng.normal(0, 1, c["b"].shape)
+    dn = rng.normal(0, 1e-3, c["n"].shape)
+    Jt, dJ, _ = tlm_misfit(c, c["b"], c["n"], db, dn, steps, obs)
+    assert abs(Jt - J) <= 1e-12 * abs(J)
+    got = float(np.dot(gb, db.reshape(-1)) + np.dot(gn, dn.reshape(-1)))
+    assert abs(got - dJ) <= 1e-8 * abs(dJ), (got, dJ)
+    adj.close()

@@ -22,6 +22,13 @@ pytestmark = pytest.mark.gpu
 REL_TOL = 1e-12          # per field per step, relative to the field's max-norm
 
 
+@pytest.fixture(autouse=True)
+def _stage_kernels(monkeypatch):
+    """These cases run on the fused stage kernel; test_parity_split_gpu.py
+    runs every one of them again on the tiled pair."""
+    monkeypatch.setenv("SWE_B200_STAGE", "fused")
+
+
 def pair(swe, **kw):
     return swe.ShallowWater(**kw), OracleSim(**kw)
 

@@ -34,6 +34,16 @@ class SweOptions(ctypes.Structure):
                 ("omega", ctypes.c_double)]
 
 
+class SweGridlands(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("cell_m", ctypes.c_double),
+                ("flip_rows", ctypes.c_int),
+                ("bed_b64", ctypes.c_char_p), ("bed_len", ctypes.c_size_t),
+                ("surface_b64", ctypes.c_char_p), ("surface_len", ctypes.c_size_t),
+                ("manning_b64", ctypes.c_char_p), ("manning_len", ctypes.c_size_t),
+                ("bed_f32", ctypes.c_void_p), ("surface_f32", ctypes.c_void_p), ("manning_f32", ctypes.c_void_p),
+                ("manning_field", ctypes.c_int)]
+
+
 class SweError(RuntimeError):
     """A failure reported by the C ABI (status code + message)."""
 
@@ -90,6 +100,16 @@ SIGNATURES = {
     "swe_hllc_batch": [_I, _DP, _DP],
     "swe_vel_batch": [_P, _I, _DP, _DP, _DP],
     "swe_max_dt_noalloc": [_I, _I, _P, _P, _P, _P, _P, _D, _D, _P, _P],
+    "swe_gridlands_decode": [ctypes.c_char_p, ctypes.c_size_t, _I, _P],
+    "swe_gridlands_create": [ctypes.POINTER(SweOptions), ctypes.POINTER(SweGridlands), ctypes.POINTER(_P)],
+    "swe_set_stage_kernels": [_P, _I],
+    "swe_get_stage_kernels": [_P, _IP],
+    "swe_render_map": [_P, _D, _D, _I, _P, _P],
+    "swe_render_tables": [_P, _P],
+    "swe_globe_lut_create": [_P, _I, _D, _D, _P, _P, _P, ctypes.POINTER(_P)],
+    "swe_globe_lut_destroy": [_P],
+    "swe_globe_lut_get": [_P, _P, _P, _P, _P, _P, _P],
+    "swe_render_globe": [_P, _P, _D, _D, _D, _I, _P, _P, _P],
     "swe_batch_create": [_I, ctypes.POINTER(SweOptions), ctypes.POINTER(_DP), ctypes.POINTER(_DP), ctypes.POINTER(_P)],
     "swe_batch_destroy": [_P],
     "swe_batch_set_boundary": [_P, _I, _I, _I],

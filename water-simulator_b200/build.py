@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libswe_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("swe_api.cu", "swe_batch.cu", "swe_adjoint.cu",
-                                                    "swe_noalloc.cu")]
+                                                    "swe_noalloc.cu", "swe_gridlands.cu", "swe_render.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("swe_kernels.cuh", "swe_math.cuh",
                                                           "swe_adjoint_math.cuh")] + [
     os.path.join(HERE, "..", "include", "swe_b200.h")]

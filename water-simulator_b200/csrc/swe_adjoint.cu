@@ -6,13 +6,15 @@
 // Forward: the bit-exact step kernels of the library, dt = maxDt() each step
 // (the dt sequence is recorded and then held fixed), the state stored every
 // `checkpoint_every` steps.  Backward: for each segment, newest first, the
-// segment's states are recomputed from its checkpoint; then each step is
-// reversed: its two stages are recomputed (same kernels, so every branch is
-// the branch the forward pass took) together with the residual's
-// intermediates (velocities, slopes, face fluxes), and the hand-written
-// reverse kernels run friction, dryClean, the stage combination, the
-// residual and the ghost-cell maps backwards.  The initial depth
-// h = max(0, eta0 - b) is part of the map from b to J.
+// segment is stepped forward again from its checkpoint (same kernels and
+// arithmetic, so every branch is the branch the forward pass took), and
+// each step's tape is kept: both stage inputs with their ghosts, both
+// positivity-limiter fields, the depths before each dryClean and friction's
+// input.  Then each step is reversed from its tape: the residual's
+// intermediates (velocities, slopes, face fluxes) are recomputed, and the
+// hand-written reverse kernels run friction, dryClean, the stage
+// combination, the residual and the ghost-cell maps backwards.  The initial
+// depth h = max(0, eta0 - b) is part of the map from b to J.
 //
 // Scope: Cartesian grids, walls (reflect) on every side, any order and
 // limiter, Coriolis, scalar or per-cell Manning n.  No sponge or Flather.
@@ -22,8 +24,10 @@
 
 #include <cuda_runtime.h>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace swe_host { void set_error(const std::string& msg); }
@@ -200,7 +204,10 @@ __global__ void k_adj_theta(Geo g, Inter it, const double* h, double dt, AdjBuf 
 
 // The faces backwards: limiter terms into the flux adjoint, then
 // face_flux's reverse.
-__global__ void k_adj_faces_core(Geo g, const double* b, const double* h, Inter it, AdjBuf a) {
+// 128 registers at most: 16 warps per SM instead of the 8 that 140 leave.
+constexpr int FACES_CORE_THREADS = 128;
+__global__ void __launch_bounds__(FACES_CORE_THREADS, 4)
+k_adj_faces_core(Geo g, const double* b, const double* h, Inter it, AdjBuf a) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
     const int i = k % g.W, j = k / g.W;
     FaceIn gx = {}, gy = {};
@@ -336,33 +343,78 @@ __global__ void k_adj_cells_final(Geo g, const double* h, const double* hu, cons
 // ---- the rest of the step backwards ----------------------------------------
 // Reflect walls: a ghost takes the clamped mirror source and flips the normal
 // momentum (src/swe.mjs:1026-1039; corners from the S/N pass).  Backwards,
-// each ghost's adjoint moves to its source; one thread walks the ghosts in a
-// fixed order so the sums are deterministic.
+// each ghost's adjoint moves to its source cell.  Every ghost has exactly one
+// source, and every source is an interior cell, so the map is a gather: one
+// thread per interior cell of the two-cell band along the edges adds the
+// ghosts that map to it, in the order of the forward fill (S/N pass by
+// column then ghost row, south before north; then the W/E pass), and zeroes
+// them.  The sums are therefore the same in every run.
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ void adj_bc_move(int W, int gi, int gj, int sk, double shu, double shv, double* lb,
+                                            double* lh, double* lhu, double* lhv, double& ab, double& ah,
+                                            double& ahu, double& ahv) {
+  const int gk = (gj + 2) * W + (gi + 2);
+  if (lb) { ab += lb[gk]; lb[gk] = 0; }
+  if (lh) {
+    ah += lh[gk]; lh[gk] = 0;
+    ahu += shu * lhu[gk]; lhu[gk] = 0;
+    ahv += shv * lhv[gk]; lhv[gk] = 0;
+  }
+  (void)sk;
+}
+
 __global__ void k_adj_bc(int nx, int ny, double* lb, double* lh, double* lhu, double* lhv) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int W = nx + 4;
-  auto clampi = [](int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); };
-  auto move = [&](int gi, int gj, int si, int sj, double shu, double shv) {
-    const int gk = (gj + 2) * W + (gi + 2), sk = (sj + 2) * W + (si + 2);
-    if (lb) { lb[sk] += lb[gk]; lb[gk] = 0; }
-    if (lh) {
-      lh[sk] += lh[gk]; lh[gk] = 0;
-      lhu[sk] += shu * lhu[gk]; lhu[gk] = 0;
-      lhv[sk] += shv * lhv[gk]; lhv[gk] = 0;
+  const int rows[4] = {0, 1, ny - 2, ny - 1};
+  const int cols[4] = {0, 1, nx - 2, nx - 1};
+  const int total = 4 * nx + 4 * ny;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    int si, sj;
+    if (t < 4 * nx) {                              // the two rows along each of S and N
+      const int r = t / nx;
+      si = t - r * nx;
+      sj = rows[r];
+      if (sj < 0 || sj > ny - 1) continue;
+      bool dup = false;
+      for (int q = 0; q < r; q++) dup |= rows[q] == sj;
+      if (dup) continue;
+    } else {                                       // the two columns along W and E, other rows
+      const int u = t - 4 * nx;
+      sj = u / 4;
+      const int c = u - 4 * sj;
+      si = cols[c];
+      if (si < 0 || si > nx - 1) continue;
+      bool dup = false;
+      for (int q = 0; q < c; q++) dup |= cols[q] == si;
+      for (int q = 0; q < 4; q++) dup |= rows[q] == sj;
+      if (dup) continue;
     }
-  };
-  for (int i = -2; i < nx + 2; i++)                 // S/N rows (final values of the corners too)
+    const int sk = (sj + 2) * W + (si + 2);
+    double ab = lb ? lb[sk] : 0, ah = 0, ahu = 0, ahv = 0;
+    if (lh) { ah = lh[sk]; ahu = lhu[sk]; ahv = lhv[sk]; }
+    // S/N pass: columns i that clamp to si, in increasing order
+    int ilist[5], ni = 0;
+    if (si == 0) { ilist[ni++] = -2; ilist[ni++] = -1; }
+    ilist[ni++] = si;
+    if (si == nx - 1) { ilist[ni++] = nx; ilist[ni++] = nx + 1; }
+    for (int q = 0; q < ni; q++) {
+      const int i = ilist[q];
+      for (int gg = 0; gg < 2; gg++) {
+        if (clampi(gg, 0, ny - 1) == sj)                       // south ghost row -1-gg
+          adj_bc_move(W, i, -1 - gg, sk, 1, -1, lb, lh, lhu, lhv, ab, ah, ahu, ahv);
+        if (clampi(ny - 1 - gg, 0, ny - 1) == sj)              // north ghost row ny+gg
+          adj_bc_move(W, i, ny + gg, sk, 1, -1, lb, lh, lhu, lhv, ab, ah, ahu, ahv);
+      }
+    }
+    // W/E pass of row sj
     for (int gg = 0; gg < 2; gg++) {
-      const int jS = -1 - gg, jN = ny + gg;
-      move(i, jS, clampi(i, 0, nx - 1), clampi(-1 - jS, 0, ny - 1), 1, -1);
-      move(i, jN, clampi(i, 0, nx - 1), clampi(2 * ny - 1 - jN, 0, ny - 1), 1, -1);
+      if (clampi(gg, 0, nx - 1) == si) adj_bc_move(W, -1 - gg, sj, sk, -1, 1, lb, lh, lhu, lhv, ab, ah, ahu, ahv);
+      if (clampi(nx - 1 - gg, 0, nx - 1) == si) adj_bc_move(W, nx + gg, sj, sk, -1, 1, lb, lh, lhu, lhv, ab, ah, ahu, ahv);
     }
-  for (int j = 0; j < ny; j++)                      // W/E columns of the interior rows
-    for (int gg = 0; gg < 2; gg++) {
-      const int iW = -1 - gg, iE = nx + gg;
-      move(iW, j, clampi(-1 - iW, 0, nx - 1), j, -1, 1);
-      move(iE, j, clampi(2 * nx - 1 - iE, 0, nx - 1), j, -1, 1);
-    }
+    if (lb) lb[sk] = ab;
+    if (lh) { lh[sk] = ah; lhu[sk] = ahu; lhv[sk] = ahv; }
+  }
 }
 
 // Stage outputs recomputed for their masks.
@@ -431,24 +483,44 @@ __global__ void k_adj_friction(int W, int H, double minDepth, double eps4, doubl
 }
 
 // J += sum_g (b + h - obs)^2 (one thread, fixed order); and its adjoint.
+// J += sum over gauges, in gauge order, of (b + h - obs)^2; eta at the gauges.
+// The loads run in parallel; one thread adds the squares in order.
+constexpr int MISFIT_THREADS = 256;
 __global__ void k_misfit(const double* b, const double* h, const int* gk, const double* obs, int ng,
                          double* J, double* eta_out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double s = *J;
-  for (int q = 0; q < ng; q++) {
-    const double e = b[gk[q]] + h[gk[q]];
-    if (eta_out) eta_out[q] = e;
-    if (obs) { const double r = e - obs[q]; s += r * r; }
+  __shared__ double r2[MISFIT_THREADS];
+  double s = 0;
+  if (threadIdx.x == 0) s = *J;
+  for (int base = 0; base < ng; base += MISFIT_THREADS) {
+    const int q = base + threadIdx.x;
+    if (q < ng) {
+      const double e = b[gk[q]] + h[gk[q]];
+      if (eta_out) eta_out[q] = e;
+      if (obs) { const double r = e - obs[q]; r2[threadIdx.x] = r * r; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && obs)
+      for (int t = 0; t < MISFIT_THREADS && base + t < ng; t++) s += r2[t];
+    __syncthreads();
   }
-  *J = s;
+  if (threadIdx.x == 0) *J = s;
 }
-__global__ void k_adj_misfit(const double* b, const double* h, const int* gk, const double* obs, int ng,
-                             double* lb, double* lh) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int q = 0; q < ng; q++) {
-    const double r = b[gk[q]] + h[gk[q]] - obs[q];
-    lh[gk[q]] += 2 * r;
-    lb[gk[q]] += 2 * r;
+// The misfit backwards: lh, lb += 2 (b + h - obs) at every gauge.  Gauges
+// that share a cell form a group, added in gauge order by one thread, so the
+// sums are those of a sequential pass over the gauges; groups run in parallel.
+__global__ void k_adj_misfit(const double* b, const double* h, const int* gcell, const int* goff, const int* gidx,
+                             int ngroups, const double* obs, double* lb, double* lh) {
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < ngroups; u += gridDim.x * blockDim.x) {
+    const int k = gcell[u];
+    const double e = b[k] + h[k];
+    double ah = lh[k], ab = lb[k];
+    for (int m = goff[u]; m < goff[u + 1]; m++) {
+      const double r = e - obs[gidx[m]];
+      ah += 2 * r;
+      ab += 2 * r;
+    }
+    lh[k] = ah;
+    lb[k] = ab;
   }
 }
 __global__ void k_set_dt(Control* ctl, const double* dts, int s) {
@@ -484,11 +556,26 @@ __global__ void k_clean_interior(int W, int H, double minDepth, const double* h,
     oh[k] = nh; ohu[k] = nhu; ohv[k] = nhv;
   }
 }
-__global__ void k_axpy(int N, double a, const double* x, double* y) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) y[k] += a * x[k];
+// The stage combinations backwards, three fields at once.
+// A = 0.5 (W1 + B + dt R2):  lB = 0.5 lA, lR = 0.5 dt lA, lA <- 0.5 lA (= lW1).
+__global__ void k_split_stage2(int N, double dt, double* lA0, double* lA1, double* lA2, double* lB0, double* lB1,
+                               double* lB2, double* lR0, double* lR1, double* lR2) {
+  const double hdt = 0.5 * dt;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double a0 = lA0[k], a1 = lA1[k], a2 = lA2[k];
+    lB0[k] = 0.5 * a0; lB1[k] = 0.5 * a1; lB2[k] = 0.5 * a2;
+    lR0[k] = hdt * a0; lR1[k] = hdt * a1; lR2[k] = hdt * a2;
+    lA0[k] = 0.5 * a0; lA1[k] = 0.5 * a1; lA2[k] = 0.5 * a2;
+  }
 }
-__global__ void k_scale(int N, double a, const double* x, double* y) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) y[k] = a * x[k];
+// B = W1 + dt R1:  lW1 += lB, lR = dt lB.
+__global__ void k_split_stage1(int N, double dt, const double* lB0, const double* lB1, const double* lB2,
+                               double* lA0, double* lA1, double* lA2, double* lR0, double* lR1, double* lR2) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    const double b0 = lB0[k], b1 = lB1[k], b2 = lB2[k];
+    lA0[k] += 1.0 * b0; lA1[k] += 1.0 * b1; lA2[k] += 1.0 * b2;
+    lR0[k] = dt * b0; lR1[k] = dt * b1; lR2[k] = dt * b2;
+  }
 }
 
 }  // namespace
@@ -500,11 +587,13 @@ struct swe_adjoint {
   cudaStream_t st = nullptr;
   std::vector<double*> allocs;
   double *b, *eta0, *nfield = nullptr, *geom;
-  double *A[3], *Bf[3], *W1[3], *Bp[3], *Ap[3], *Adc[3];  // state, stage buffers
-  double *R[4];                                           // rh rhu rhv theta
-  double *ckpt, *seg;                                     // checkpoints, one segment of states
+  double *A[3], *Bf[3], *X[3], *Ap[3], *Adc[3];           // state, stage buffers
+  double *R[4];                                           // residual scratch
+  double *ckpt, *tape;                                    // checkpoints, one segment's tapes
   double *dts, *obs = nullptr, *J, *eta_series = nullptr;
   int* gk;
+  int* gmeta = nullptr;          // gauge groups by cell: cells, offsets, gauge indices
+  int ngroups = 0;
   double *lA[3], *lB[3], *lb, *ln;
   Inter it;
   AdjBuf ab;
@@ -514,6 +603,7 @@ struct swe_adjoint {
   dim3 grid;
   bool forward_done = false;
   bool fixed_dt = false;         // forward uses the given dt sequence instead of maxDt()
+  std::vector<double> dts_host;  // the dt sequence, read once per backward pass
 };
 
 namespace {
@@ -560,6 +650,7 @@ BCArgs bc_args(const swe_adjoint* s, double* const* f) {
 
 int G1(const swe_adjoint* s) { return std::min(4096, (s->N + 255) / 256); }
 int bcb(const swe_adjoint* s) { return (4 * s->o.ny + 4 * (s->o.nx + 4) + 255) / 256; }
+int adjbc_blocks(const swe_adjoint* s) { return (4 * s->o.nx + 4 * s->o.ny + 255) / 256; }
 
 // One forward step of state X in place, dt from the device control block
 // (set by k_set_dt or, when auto_dt, from the CFL rate).
@@ -596,77 +687,96 @@ int residual_adjoint(swe_adjoint* s, double* const* X, const double* theta, doub
   k_faces<<<gb, 256, 0, s->st>>>(g, s->b, X[0], s->it);
   k_adj_faces_accum<<<gb, 256, 0, s->st>>>(g, s->it, theta, s->ab);
   k_adj_theta<<<gb, 256, 0, s->st>>>(g, s->it, X[0], dt, s->ab);
-  k_adj_faces_core<<<gb, 256, 0, s->st>>>(g, s->b, X[0], s->it, s->ab);
+  k_adj_faces_core<<<std::min(148 * 4 * 4, (s->N + FACES_CORE_THREADS - 1) / FACES_CORE_THREADS),
+                     FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], s->it, s->ab);
   k_adj_cells<<<gb, 256, 0, s->st>>>(g, s->b, X[0], X[1], X[2], s->it, s->ab, lX[1], lX[2]);
   k_adj_cells_final<<<gb, 256, 0, s->st>>>(g, X[0], X[1], X[2], s->it, s->ab, s->lb, lX[0], lX[1], lX[2]);
   CU(cudaGetLastError());
   return SWE_OK;
 }
 
-// Reverse one step: on entry lA holds the adjoint of the step's output
-// (interior), on exit the adjoint of its input state X0 (interior); lb and
-// ln accumulate.
-int step_adjoint(swe_adjoint* s, double* const* X0, int sidx) {
+// One step's tape: what the reverse of the step reads.  The segment pass
+// writes it while stepping forward from the segment's checkpoint; the step
+// is the same arithmetic as the fused kernels (their updates are these
+// elementwise expressions, their residual is k_stage<0>), so the states are
+// the forward pass's own.
+struct Tape {
+  double* W1[3];   // stage-1 input with ghosts filled
+  double* th1;     // positivity limiter of stage 1
+  double* hB;      // stage-1 depth before dryClean
+  double* Bp[3];   // stage-2 input with ghosts filled
+  double* th2;     // positivity limiter of stage 2
+  double* hA;      // stage-2 depth before dryClean
+  double* Bf[3];   // friction's input
+  double* hX;      // the step's output depth (the misfit reads it)
+};
+constexpr int TAPE_FIELDS = 14;
+
+Tape tape_at(const swe_adjoint* s, int t) {
+  double* p = s->tape + (size_t)t * TAPE_FIELDS * s->N;
+  const size_t N = s->N;
+  Tape T;
+  for (int q = 0; q < 3; q++) { T.W1[q] = p + q * N; T.Bp[q] = p + (5 + q) * N; T.Bf[q] = p + (10 + q) * N; }
+  T.th1 = p + 3 * N; T.hB = p + 4 * N; T.th2 = p + 8 * N; T.hA = p + 9 * N; T.hX = p + 13 * N;
+  return T;
+}
+
+// Step k forward from X (in place) and record its tape.
+int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
   const int N = s->N, gb = G1(s);
+  const double dt = s->dts_host[k];
+  k_set_dt<<<1, 32, 0, s->st>>>(s->ctl, s->dts, k);
+  double* Bpre[3] = {T.hB, s->Adc[1], s->Adc[2]};
+  double* Apre[3] = {T.hA, s->Ap[1], s->Ap[2]};
+  copy3(s, T.W1, X);
+  swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, T.W1), s->ctl, 0);
+  StageArgs r1 = stage_args(s, T.W1, nullptr);
+  r1.rh = s->R[0]; r1.rhu = s->R[1]; r1.rhv = s->R[2]; r1.theta = T.th1;
+  swe::k_stage<0><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(r1, s->ctl);
+  k_stage1_pre<<<gb, 256, 0, s->st>>>(N, T.W1[0], T.W1[1], T.W1[2], s->R[0], s->R[1], s->R[2], dt,
+                                      Bpre[0], Bpre[1], Bpre[2]);
+  k_clean_interior<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, Bpre[0], Bpre[1], Bpre[2],
+                                          T.Bp[0], T.Bp[1], T.Bp[2]);
+  swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, T.Bp), s->ctl, 0);
+  StageArgs r2 = stage_args(s, T.Bp, nullptr);
+  r2.rh = s->R[0]; r2.rhu = s->R[1]; r2.rhv = s->R[2]; r2.theta = T.th2;
+  swe::k_stage<0><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(r2, s->ctl);
+  k_stage2_pre<<<gb, 256, 0, s->st>>>(N, T.W1[0], T.W1[1], T.W1[2], T.Bp[0], T.Bp[1], T.Bp[2],
+                                      s->R[0], s->R[1], s->R[2], dt, Apre[0], Apre[1], Apre[2]);
+  k_clean_interior<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, Apre[0], Apre[1], Apre[2],
+                                          T.Bf[0], T.Bf[1], T.Bf[2]);
+  copy3(s, X, T.Bf);
+  StageArgs fr = stage_args(s, X, X);
+  swe::k_friction<<<std::max(1, std::min(4096, (s->o.nx * s->o.ny + 255) / 256)), 256, 0, s->st>>>(fr, dt);
+  cudaMemcpyAsync(T.hX, X[0], sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
+  CU(cudaGetLastError());
+  return SWE_OK;
+}
+
+// Reverse step k: on entry lA holds the adjoint of the step's output
+// (interior), on exit the adjoint of its input (interior); lb and ln
+// accumulate.
+int reverse_step(swe_adjoint* s, int k, const Tape& T) {
+  const int N = s->N, gb = G1(s);
+  const double dt = s->dts_host[k];
   double* lA[3] = {s->lA[0], s->lA[1], s->lA[2]};
   double* lB[3] = {s->lB[0], s->lB[1], s->lB[2]};
-  double dt_h;
-  CU(cudaMemcpyAsync(&dt_h, s->dts + sidx, sizeof(double), cudaMemcpyDeviceToHost, s->st));
-  CU(cudaStreamSynchronize(s->st));
-  const double dt = dt_h;
-  k_set_dt<<<1, 32, 0, s->st>>>(s->ctl, s->dts, sidx);
-  // recompute: W1 = BC(X0); R1; B pre/post clean; Bp = BC(B); R2; A pre/post clean
-  copy3(s, s->W1, X0);
-  swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, s->W1), s->ctl, 0);
-  StageArgs r1 = stage_args(s, s->W1, nullptr);
-  r1.rh = s->R[0]; r1.rhu = s->R[1]; r1.rhv = s->R[2]; r1.theta = s->R[3];
-  swe::k_stage<0><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(r1, s->ctl);
-  k_stage1_pre<<<gb, 256, 0, s->st>>>(N, s->W1[0], s->W1[1], s->W1[2], s->R[0], s->R[1], s->R[2], dt,
-                                      s->Ap[0], s->Ap[1], s->Ap[2]);            // Ap = B before dryClean
-  // stage-1 output after dryClean = the fused kernel's B
-  swe::k_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(stage_args(s, s->W1, s->Bf), s->ctl);
-  copy3(s, s->Bp, s->Bf);
-  swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, s->Bp), s->ctl, 0);
-  // B before clean is needed for the stage-1 mask: keep it in Adc for now
-  copy3(s, s->Adc, s->Ap);
-  StageArgs r2 = stage_args(s, s->Bp, nullptr);
-  r2.rh = s->R[0]; r2.rhu = s->R[1]; r2.rhv = s->R[2]; r2.theta = s->R[3];
-  swe::k_stage<0><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(r2, s->ctl);
-  k_stage2_pre<<<gb, 256, 0, s->st>>>(N, s->W1[0], s->W1[1], s->W1[2], s->Bp[0], s->Bp[1], s->Bp[2],
-                                      s->R[0], s->R[1], s->R[2], dt, s->Ap[0], s->Ap[1], s->Ap[2]);
-  // post-clean stage-2 state (friction's input): the fused kernel without friction
-  // is not exposed, so clean Ap's copy here exactly as dryClean does
-  CU(cudaGetLastError());
-  {
-    // Bf <- Ap cleaned (Bf is free now: stage 2's input lives in Bp)
-    k_clean_interior<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, s->Ap[0], s->Ap[1], s->Ap[2],
-                                            s->Bf[0], s->Bf[1], s->Bf[2]);
-  }
-  // ---- reverse ----
   k_adj_friction<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, s->eps4, s->o.manning, s->nfield, dt,
-                                        s->Bf[0], s->Bf[1], s->Bf[2], lA[0], lA[1], lA[2], s->ln);
-  k_adj_dryclean<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, s->Ap[0], lA[0], lA[1], lA[2]);
-  // A = 0.5 (W1 + Bp + dt R2): lW1 = lB = 0.5 lA, lR2 = 0.5 dt lA
-  for (int q = 0; q < 3; q++) {
-    k_scale<<<gb, 256, 0, s->st>>>(N, 0.5, lA[q], lB[q]);
-    k_scale<<<gb, 256, 0, s->st>>>(N, 0.5 * dt, lA[q], s->ab.lR[q]);
-    k_scale<<<gb, 256, 0, s->st>>>(N, 0.5, lA[q], lA[q]);       // lA now holds lW1
-  }
-  int rc = residual_adjoint(s, s->Bp, s->R[3], dt, lB);
+                                        T.Bf[0], T.Bf[1], T.Bf[2], lA[0], lA[1], lA[2], s->ln);
+  k_adj_dryclean<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, T.hA, lA[0], lA[1], lA[2]);
+  // A = 0.5 (W1 + Bp + dt R2): lB = 0.5 lA, lR2 = 0.5 dt lA, lW1 = 0.5 lA
+  k_split_stage2<<<gb, 256, 0, s->st>>>(N, dt, lA[0], lA[1], lA[2], lB[0], lB[1], lB[2], s->ab.lR[0],
+                                        s->ab.lR[1], s->ab.lR[2]);
+  int rc = residual_adjoint(s, T.Bp, T.th2, dt, lB);
   if (rc) return rc;
-  k_adj_bc<<<1, 32, 0, s->st>>>(s->o.nx, s->o.ny, s->lb, lB[0], lB[1], lB[2]);
-  // stage-1 dryClean backwards (mask from B before clean, kept in Adc)
-  k_adj_dryclean<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, s->Adc[0], lB[0], lB[1], lB[2]);
+  k_adj_bc<<<adjbc_blocks(s), 256, 0, s->st>>>(s->o.nx, s->o.ny, s->lb, lB[0], lB[1], lB[2]);
+  k_adj_dryclean<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, T.hB, lB[0], lB[1], lB[2]);
   // B = W1 + dt R1 (all cells): lW1 += lB, lR1 = dt lB
-  StageArgs r1b = r1;
-  swe::k_stage<0><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(r1b, s->ctl);   // theta of stage 1
-  for (int q = 0; q < 3; q++) {
-    k_axpy<<<gb, 256, 0, s->st>>>(N, 1.0, lB[q], lA[q]);
-    k_scale<<<gb, 256, 0, s->st>>>(N, dt, lB[q], s->ab.lR[q]);
-  }
-  rc = residual_adjoint(s, s->W1, s->R[3], dt, lA);
+  k_split_stage1<<<gb, 256, 0, s->st>>>(N, dt, lB[0], lB[1], lB[2], lA[0], lA[1], lA[2], s->ab.lR[0],
+                                        s->ab.lR[1], s->ab.lR[2]);
+  rc = residual_adjoint(s, T.W1, T.th1, dt, lA);
   if (rc) return rc;
-  k_adj_bc<<<1, 32, 0, s->st>>>(s->o.nx, s->o.ny, s->lb, lA[0], lA[1], lA[2]);
+  k_adj_bc<<<adjbc_blocks(s), 256, 0, s->st>>>(s->o.nx, s->o.ny, s->lb, lA[0], lA[1], lA[2]);
   CU(cudaGetLastError());
   return SWE_OK;
 }
@@ -674,6 +784,7 @@ int step_adjoint(swe_adjoint* s, double* const* X0, int sidx) {
 void free_adj(swe_adjoint* s) {
   for (double* p : s->allocs) cudaFree(p);
   if (s->gk) cudaFree(s->gk);
+  if (s->gmeta) cudaFree(s->gmeta);
   if (s->ctl) cudaFree(s->ctl);
   if (s->st) cudaStreamDestroy(s->st);
 }
@@ -715,12 +826,12 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
   s->b = A(N); s->eta0 = A(N); s->geom = A((SWE_GEOM_NROWS + 3) * (size_t)s->H);
   if (manning_field) s->nfield = A(N);
   for (int q = 0; q < 3; q++) {
-    s->A[q] = A(N); s->Bf[q] = A(N); s->W1[q] = A(N); s->Bp[q] = A(N); s->Ap[q] = A(N); s->Adc[q] = A(N);
+    s->A[q] = A(N); s->Bf[q] = A(N); s->X[q] = A(N); s->Ap[q] = A(N); s->Adc[q] = A(N);
     s->lA[q] = A(N); s->lB[q] = A(N);
   }
   for (int q = 0; q < 4; q++) s->R[q] = A(N);
   s->ckpt = A(3 * N * (size_t)s->nseg);
-  s->seg = A(3 * N * (size_t)(checkpoint_every + 1));
+  s->tape = nullptr;               // allocated by the first backward pass
   s->dts = A(steps);
   s->obs = A((size_t)steps * n_gauges);
   s->eta_series = A((size_t)steps * n_gauges);
@@ -756,6 +867,34 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
   cudaMemcpyAsync(s->eta0, eta0, sizeof(double) * N, cudaMemcpyHostToDevice, s->st);
   if (manning_field) cudaMemcpyAsync(s->nfield, manning_field, sizeof(double) * N, cudaMemcpyHostToDevice, s->st);
   cudaMemcpyAsync(s->gk, gauge_cells, sizeof(int) * n_gauges, cudaMemcpyHostToDevice, s->st);
+  {
+    // group the gauges by cell, groups in order of first appearance
+    std::vector<int> cells;
+    std::vector<std::vector<int>> members;
+    std::unordered_map<int, int> group_of;
+    for (int q = 0; q < n_gauges; q++) {
+      auto it = group_of.find(gauge_cells[q]);
+      int u;
+      if (it == group_of.end()) {
+        u = (int)cells.size();
+        group_of.emplace(gauge_cells[q], u);
+        cells.push_back(gauge_cells[q]);
+        members.emplace_back();
+      } else {
+        u = it->second;
+      }
+      members[u].push_back(q);
+    }
+    s->ngroups = (int)cells.size();
+    std::vector<int> meta(cells);
+    meta.push_back(0);
+    for (auto& m : members) meta.push_back(meta.back() + (int)m.size());
+    for (auto& m : members) meta.insert(meta.end(), m.begin(), m.end());
+    if (cudaMalloc(&s->gmeta, sizeof(int) * meta.size()) != cudaSuccess)
+      return bail(fail(SWE_ECUDA, "swe_adjoint_create: out of device memory"));
+    cudaMemcpyAsync(s->gmeta, meta.data(), sizeof(int) * meta.size(), cudaMemcpyHostToDevice, s->st);
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) return bail(fail(SWE_ECUDA, "swe_adjoint_create: upload"));
+  }
   if (cudaStreamSynchronize(s->st) != cudaSuccess) return bail(fail(SWE_ECUDA, "swe_adjoint_create: upload"));
   *out = s;
   return SWE_OK;
@@ -794,7 +933,7 @@ int swe_adjoint_forward(swe_adjoint* s, double* J, double* gauge_eta) {
     }
     int rc = fwd_step(s, s->A, !s->fixed_dt, k);
     if (rc) return rc;
-    k_misfit<<<1, 32, 0, s->st>>>(s->b, s->A[0], s->gk, s->obs + (size_t)k * s->ng, s->ng, s->J,
+    k_misfit<<<1, MISFIT_THREADS, 0, s->st>>>(s->b, s->A[0], s->gk, s->obs + (size_t)k * s->ng, s->ng, s->J,
                                   s->eta_series + (size_t)k * s->ng);
   }
   CU(cudaGetLastError());
@@ -813,28 +952,36 @@ int swe_adjoint_backward(swe_adjoint* s, double* grad_b, double* grad_n) {
   for (int q = 0; q < 3; q++) CU(cudaMemsetAsync(s->lA[q], 0, sizeof(double) * N, s->st));
   CU(cudaMemsetAsync(s->lb, 0, sizeof(double) * N, s->st));
   CU(cudaMemsetAsync(s->ln, 0, sizeof(double) * N, s->st));
-  auto slot = [&](int i) {
-    double* p = s->seg + (size_t)i * 3 * N;
-    return std::vector<double*>{p, p + N, p + 2 * N};
-  };
+  if (!s->tape) {
+    const size_t bytes = sizeof(double) * TAPE_FIELDS * N * (size_t)std::min(s->every, s->steps);
+    if (cudaMalloc(&s->tape, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      s->tape = nullptr;
+      char buf[200];
+      std::snprintf(buf, sizeof buf, "swe_adjoint_backward: the tape of one segment (%.2f GB) does not fit on "
+                    "the device; use a smaller checkpoint_every", bytes / 1e9);
+      return fail(SWE_ECUDA, buf);
+    }
+    s->allocs.push_back(s->tape);
+  }
+  s->dts_host.assign(s->steps, 0.0);
+  CU(cudaMemcpyAsync(s->dts_host.data(), s->dts, sizeof(double) * s->steps, cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
   for (int sg = s->nseg - 1; sg >= 0; sg--) {
     const int k0 = sg * s->every, k1 = std::min(s->steps, k0 + s->every);
-    // states A_k0 .. A_k1 of this segment
-    {
-      auto d0 = slot(0);
-      double* src[3] = {s->ckpt + (size_t)sg * 3 * N, s->ckpt + ((size_t)sg * 3 + 1) * N, s->ckpt + ((size_t)sg * 3 + 2) * N};
-      copy3(s, d0.data(), src);
-    }
+    // the segment forward from its checkpoint, recording each step's tape
+    double* src[3] = {s->ckpt + (size_t)sg * 3 * N, s->ckpt + ((size_t)sg * 3 + 1) * N, s->ckpt + ((size_t)sg * 3 + 2) * N};
+    copy3(s, s->X, src);
     for (int k = k0; k < k1; k++) {
-      auto cur = slot(k - k0), nxt = slot(k - k0 + 1);
-      copy3(s, nxt.data(), cur.data());
-      int rc = fwd_step(s, nxt.data(), false, k);
+      int rc = tape_step(s, s->X, k, tape_at(s, k - k0));
       if (rc) return rc;
     }
     for (int k = k1 - 1; k >= k0; k--) {
-      auto outp = slot(k - k0 + 1), inp = slot(k - k0);
-      k_adj_misfit<<<1, 32, 0, s->st>>>(s->b, outp[0], s->gk, s->obs + (size_t)k * s->ng, s->ng, s->lb, s->lA[0]);
-      int rc = step_adjoint(s, inp.data(), k);
+      const Tape T = tape_at(s, k - k0);
+      k_adj_misfit<<<(s->ngroups + 127) / 128, 128, 0, s->st>>>(
+          s->b, T.hX, s->gmeta, s->gmeta + s->ngroups, s->gmeta + 2 * s->ngroups + 1, s->ngroups,
+          s->obs + (size_t)k * s->ng, s->lb, s->lA[0]);
+      int rc = reverse_step(s, k, T);
       if (rc) return rc;
     }
   }

@@ -5,6 +5,7 @@
 // update runs on the GPU.
 #include "../../include/swe_b200.h"
 #include "swe_kernels.cuh"
+#include "swe_split.cuh"
 
 #include <cuda_runtime.h>
 #include <cmath>
@@ -44,6 +45,13 @@ double cos_lat(double p) {                                                      
 
 }  // namespace
 
+// The tiled pair measured faster than the fused kernel on every workload
+// tried (2048^2 beach and all-wet, 1024^2, the 1440x720 sphere), with the
+// same results bit for bit.
+#ifndef SWE_DEFAULT_STAGE
+#define SWE_DEFAULT_STAGE 1
+#endif
+
 namespace swe_host {
 // Lets the other translation unit of the library report through swe_last_error().
 void set_error(const std::string& msg) { g_err = msg; }
@@ -80,11 +88,38 @@ struct swe_sim {
   int nblocks = 0;
   int part_cap = 0;
   // device-resident loop graph
+  // stage kernels: 0 the fused row-marching kernel, 1 the two tiled kernels
+  int stage_impl = 0;
+  double* d_split = nullptr;
+  swe::SplitBufs sb;
+  dim3 sgrid;
   cudaGraphExec_t gexec = nullptr;
   int g_steps = 0, g_mode = -1;
   double g_dt = 0, g_tend = 0;
   unsigned long long g_version = 0, version = 1;
 };
+
+namespace swe_host {
+cudaStream_t stream_of(swe_sim* s) { return s->st; }
+
+// Take b, h (and a Manning field, or none) from device arrays over the padded
+// grid, in the handle's stream; used by importers that build the fields on
+// the device.
+int adopt_fields(swe_sim* s, const double* d_b, const double* d_h, const double* d_n) {
+  const size_t nb = sizeof(double) * (size_t)s->N;
+  cudaError_t e = cudaMemcpyAsync(s->d_b, d_b, nb, cudaMemcpyDeviceToDevice, s->st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_A[0], d_h, nb, cudaMemcpyDeviceToDevice, s->st);
+  if (e == cudaSuccess && d_n) {
+    if (!s->d_nfield) e = cudaMalloc(&s->d_nfield, nb);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_nfield, d_n, nb, cudaMemcpyDeviceToDevice, s->st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) { set_error(std::string("adopt_fields: ") + cudaGetErrorString(e)); return SWE_ECUDA; }
+  s->version++;
+  s->cfl_valid = false;
+  return SWE_OK;
+}
+}  // namespace swe_host
 
 namespace {
 
@@ -235,6 +270,31 @@ int launch_bc(swe_sim* s, double* const* f, int respect_stop) {
 }
 
 // One SSP-RK2 step on the device; `mode`/`dt`/`t_end` as k_prepare.
+// Buffers of the tiled stage kernels (faces and source terms, 14 fields).
+int ensure_split(swe_sim* s) {
+  if (s->d_split) return SWE_OK;
+  const size_t N = s->N;
+  CU(cudaMalloc(&s->d_split, sizeof(double) * 14 * N));
+  CU(cudaMemsetAsync(s->d_split, 0, sizeof(double) * 14 * N, s->st));
+  for (int q = 0; q < 5; q++) { s->sb.fx[q] = s->d_split + q * N; s->sb.fy[q] = s->d_split + (5 + q) * N; }
+  for (int q = 0; q < 3; q++) s->sb.tb[q] = s->d_split + (10 + q) * N;
+  s->sb.U = s->d_split + 13 * N;
+  return SWE_OK;
+}
+
+// One stage (MODE 1 or 2) with the selected kernels.
+template <int MODE>
+int launch_stage(swe_sim* s, const swe::StageArgs& a) {
+  if (s->stage_impl == 1) {
+    swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, s->sb, s->d_ctl);
+    swe::k_split_cells<MODE><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, s->sb, s->d_ctl);
+  } else {
+    swe::k_stage<MODE><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a, s->d_ctl);
+  }
+  CU(cudaGetLastError());
+  return SWE_OK;
+}
+
 int enqueue_step(swe_sim* s, int mode, double dt, double t_end) {
   swe::k_prepare<<<1, 32, 0, s->st>>>(s->d_ctl, prep_args(s, mode, dt, t_end));
   CU(cudaGetLastError());
@@ -244,15 +304,13 @@ int enqueue_step(swe_sim* s, int mode, double dt, double t_end) {
   int rc = launch_bc(s, s->d_A, mode == 0 ? 0 : 1);
   if (rc) return rc;
   swe::StageArgs a1 = stage_args(s, s->d_A, s->d_B);
-  swe::k_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a1, s->d_ctl);
-  CU(cudaGetLastError());
+  rc = launch_stage<1>(s, a1);
+  if (rc) return rc;
   rc = launch_bc(s, s->d_B, 1);
   if (rc) return rc;
   swe::StageArgs a2 = stage_args(s, s->d_B, s->d_A);
   if (s->keep_h0) { a2.h0c = s->d_h0[0]; a2.hu0c = s->d_h0[1]; a2.hv0c = s->d_h0[2]; }
-  swe::k_stage<2><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a2, s->d_ctl);
-  CU(cudaGetLastError());
-  return SWE_OK;
+  return launch_stage<2>(s, a2);
 }
 
 int ensure_cfl(swe_sim* s) {
@@ -299,6 +357,21 @@ double* field_ptr(swe_sim* s, int f) {
   }
 }
 
+}  // namespace
+
+namespace swe_host {
+// Read-only view of a handle for the other translation units (frames).
+void view_of(swe_sim* s, int* dims, double* opts, const double** b, const double** h, cudaStream_t* st) {
+  dims[0] = s->nx; dims[1] = s->ny; dims[2] = s->W; dims[3] = s->H; dims[4] = s->o.sphere;
+  opts[0] = s->o.min_depth; opts[1] = s->o.lat0; opts[2] = s->o.lat1; opts[3] = s->dx; opts[4] = s->dy;
+  *b = field_ptr(s, SWE_FIELD_B);
+  *h = field_ptr(s, SWE_FIELD_H);
+  *st = s->st;
+}
+}  // namespace swe_host
+
+namespace {
+
 // Reciprocals of the three flux divisors (rows after the 13 metric rows).
 void fill_reciprocals(swe_sim* s) {
   const int src[3] = {SWE_GEOM_DXROW, SWE_GEOM_DYROWN, SWE_GEOM_DYROWS};
@@ -323,7 +396,8 @@ void free_all(swe_sim* s) {
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
   double** ptrs[] = {&s->d_b, &s->d_A[0], &s->d_A[1], &s->d_A[2], &s->d_B[0], &s->d_B[1], &s->d_B[2],
                      &s->d_h0[0], &s->d_h0[1], &s->d_h0[2], &s->d_res[0], &s->d_res[1], &s->d_res[2],
-                     &s->d_res[3], &s->d_nfield, &s->d_geom, &s->d_part, &s->d_rows, &s->d_sponge};
+                     &s->d_res[3], &s->d_nfield, &s->d_geom, &s->d_part, &s->d_rows, &s->d_sponge,
+                     &s->d_split};
   for (double** p : ptrs) if (*p) { cudaFree(*p); *p = nullptr; }
   if (s->d_ctl) cudaFree(s->d_ctl);
   if (s->st) cudaStreamDestroy(s->st);
@@ -388,7 +462,8 @@ int swe_create(const swe_options* o, const double* b, const double* h, swe_sim**
   const int gy = (s->H + ry - 1) / ry;
   s->grid = dim3(gx, gy, 1);
   s->nblocks = gx * gy;
-  s->part_cap = std::max(s->nblocks, 1024);
+  s->sgrid = dim3((s->W + swe::SPX - 1) / swe::SPX, (s->H + swe::SPY - 1) / swe::SPY, 1);
+  s->part_cap = std::max(std::max(s->nblocks, (int)(s->sgrid.x * s->sgrid.y)), 1024);
 
   auto bail = [&](int rc) { free_all(s); delete s; return rc; };
   const size_t nb = sizeof(double) * (size_t)s->N;
@@ -417,6 +492,12 @@ int swe_create(const swe_options* o, const double* b, const double* h, swe_sim**
   else CUB(cudaMemsetAsync(s->d_b, 0, nb, s->st));
   if (h) CUB(cudaMemcpyAsync(s->d_A[0], h, nb, cudaMemcpyHostToDevice, s->st));
   if (upload_geom(s)) return bail(SWE_ECUDA);
+  {
+    const char* env = std::getenv("SWE_B200_STAGE");
+    s->stage_impl = (env && std::strcmp(env, "fused") == 0) ? 0 : (env && std::strcmp(env, "split") == 0) ? 1
+                                                                  : SWE_DEFAULT_STAGE;
+    if (s->stage_impl == 1 && ensure_split(s)) return bail(SWE_ECUDA);
+  }
   CUB(cudaStreamSynchronize(s->st));
 #undef CUB
   *out = s;
@@ -853,14 +934,16 @@ int swe_step_timed(swe_sim* s, double dt, double* ms) {
   rc = launch_bc(s, s->d_A, 0);
   if (rc) return rc;
   CU(cudaEventRecord(ev[2], s->st));
-  swe::k_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(stage_args(s, s->d_A, s->d_B), s->d_ctl);
+  rc = launch_stage<1>(s, stage_args(s, s->d_A, s->d_B));
+  if (rc) return rc;
   CU(cudaEventRecord(ev[3], s->st));
   rc = launch_bc(s, s->d_B, 1);
   if (rc) return rc;
   CU(cudaEventRecord(ev[4], s->st));
   swe::StageArgs a2 = stage_args(s, s->d_B, s->d_A);
   if (s->keep_h0) { a2.h0c = s->d_h0[0]; a2.hu0c = s->d_h0[1]; a2.hv0c = s->d_h0[2]; }
-  swe::k_stage<2><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a2, s->d_ctl);
+  rc = launch_stage<2>(s, a2);
+  if (rc) return rc;
   CU(cudaEventRecord(ev[5], s->st));
   CU(cudaEventSynchronize(ev[5]));
   for (int q = 0; q < 5; q++) {
@@ -877,8 +960,31 @@ int swe_step_timed(swe_sim* s, double dt, double* ms) {
 
 int swe_get_launch_config(swe_sim* s, int* cfg) {
   if (!s || !cfg) return fail(SWE_EINVAL, "null argument");
-  cfg[0] = (int)s->grid.x; cfg[1] = (int)s->grid.y; cfg[2] = swe::BX; cfg[3] = swe::SX;
-  cfg[4] = (s->H + (int)s->grid.y - 1) / (int)s->grid.y;
+  if (s->stage_impl == 1) {
+    cfg[0] = (int)s->sgrid.x; cfg[1] = (int)s->sgrid.y; cfg[2] = swe::SP_THREADS; cfg[3] = swe::SPX;
+    cfg[4] = swe::SPY;
+  } else {
+    cfg[0] = (int)s->grid.x; cfg[1] = (int)s->grid.y; cfg[2] = swe::BX; cfg[3] = swe::SX;
+    cfg[4] = (s->H + (int)s->grid.y - 1) / (int)s->grid.y;
+  }
+  return SWE_OK;
+}
+
+int swe_set_stage_kernels(swe_sim* s, int impl) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (impl != SWE_STAGE_FUSED && impl != SWE_STAGE_SPLIT) return fail(SWE_EINVAL, "unknown stage kernels");
+  if (impl == SWE_STAGE_SPLIT) {
+    int rc = ensure_split(s);
+    if (rc) return rc;
+  }
+  s->stage_impl = impl;
+  s->version++;                     // the cached graph holds the other kernels
+  return SWE_OK;
+}
+
+int swe_get_stage_kernels(swe_sim* s, int* impl) {
+  if (!s || !impl) return fail(SWE_EINVAL, "null argument");
+  *impl = s->stage_impl;
   return SWE_OK;
 }
 

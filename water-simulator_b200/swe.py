@@ -212,7 +212,7 @@ class ShallowWater:
     """new ShallowWater({...}) of src/swe.mjs:170-244, on the GPU."""
 
     def __init__(self, nx, ny, dx=None, dy=None, bed=None, eta0=0, manning=0.025, minDepth=1e-3,
-                 cfl=0.45, coriolis=0, order=2, limiter="mc", sphere=None):
+                 cfl=0.45, coriolis=0, order=2, limiter="mc", sphere=None, _gridlands_manning=False):
         lib = _lib.load()
         self._lib = lib
         if limiter not in LIMITERS:
@@ -241,12 +241,19 @@ class ShallowWater:
             coords = lambda i, j: self.cellCentre(i - 2, j - 2)
         if bed is None:
             bed = 0.0
-        b = _sample(bed, coords, shape).reshape(-1)
-        e = _sample(eta0, coords, shape).reshape(-1)
-        h = _jmax0(e - b)
-        handle = ctypes.c_void_p()
-        check(lib.swe_create(ctypes.byref(o), dptr(b), dptr(h), ctypes.byref(handle)))
-        self._h = handle
+        terrain = getattr(bed, "_gridlands", None)
+        if terrain is not None and not sphere and getattr(eta0, "_gridlands", None) is terrain \
+                and bed is terrain.bed and eta0 is terrain.eta0:
+            # an imported gridlands terrain: sampled on the device from its layers
+            from .gridlands import create_sim_handle
+            self._h = create_sim_handle(o, terrain, manning_field=_gridlands_manning)
+        else:
+            b = _sample(bed, coords, shape).reshape(-1)
+            e = _sample(eta0, coords, shape).reshape(-1)
+            h = _jmax0(e - b)
+            handle = ctypes.c_void_p()
+            check(lib.swe_create(ctypes.byref(o), dptr(b), dptr(h), ctypes.byref(handle)))
+            self._h = handle
         # host mirrors
         self._host = {}
         self._fresh = set()
@@ -257,6 +264,22 @@ class ShallowWater:
         self._boundaries = _Boundaries(self, sphere is not None and sphere is not False)
         self._apply_boundaries_kinds()
         self._sponge = None
+
+        if terrain is not None and _gridlands_manning:
+            nf = np.empty(self.W * self.H)
+            check(lib.swe_get_field(self._h, FIELD["manning"], dptr(nf)))
+            self.manningField = nf
+
+    @classmethod
+    def fromGridlands(cls, t, manningField=False, **opts):
+        """new ShallowWater({nx, ny, dx, dy from t.domain, bed: t.bed, eta0: t.eta0,
+        manning: t.manning, ...opts}) for a terrain from gridlandsTerrain(), built
+        on the device; with manningField, the export's per-cell n as well (the
+        field tools/verify-gridlands.mjs:326-333 sets)."""
+        d = t.domain
+        kw = dict(nx=d["nx"], ny=d["ny"], dx=d["dx"], dy=d["dy"], manning=t.manning)
+        kw.update(opts)
+        return cls(bed=t.bed, eta0=t.eta0, _gridlands_manning=bool(manningField), **kw)
 
     # ---- lifetime -----------------------------------------------------------
     def close(self):

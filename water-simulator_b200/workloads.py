@@ -126,3 +126,48 @@ def adjoint_case(nx=1024, ny=1024, dx=10.0, n_gauges=32, seed=5, hump=0.5, noise
     gauges = (gj * W + gi).astype(np.int32)
     b_true = b + rng.normal(0.0, noise, X.shape)
     return {"nx": nx, "ny": ny, "dx": dx, "b": b, "b_true": b_true, "eta0": eta0, "n": n, "gauges": gauges}
+
+
+def _legendre(n, x):
+    """P_n(x) by Bonnet's recurrence (n + 1) P_{n+1} = (2n + 1) x P_n - n P_{n-1}."""
+    p0, p1 = np.ones_like(x), x
+    if n == 0:
+        return p0
+    for k in range(1, n):
+        p0, p1 = p1, ((2 * k + 1) * x * p1 - k * p0) / (k + 1)
+    return p1
+
+
+def globe_tide(nx=1440, ny=720, lat0=-85.0, lat1=85.0, seed=3, land=0.30, depth=5000.0, land_height=50.0,
+               modes=48):
+    """The spherical tide workload: 1440 x 720 cells on the lat-lon grid
+    (0.25 degrees in longitude) over the band lat0..lat1, whose south and
+    north edges are the open boundaries the tide enters through (the whole
+    sphere has none: longitude is periodic and the pole faces have zero
+    length).  Bed: band-limited spherical noise, the sum of `modes` seeded
+    terms P_k(sin lat) cos(m lon + p) with degrees k and zonal wavenumbers
+    m in 1..12 (periodic across the seam), scaled so the ocean spans depths
+    0..`depth` m; the `land` fraction of highest cells is land at
+    +`land_height` m.  Still water at 0.  Returns padded arrays b, eta0 and
+    the cell centres (lon, lat) in degrees, longitude wrapped into
+    [-180, 180) as cellLonLat does."""
+    W, H = nx + 4, ny + 4
+    dlon, dlat = 360.0 / nx, (lat1 - lat0) / ny
+    lon = -180.0 + (np.arange(W) - 2 + 0.5) * dlon
+    lon = (lon + 180.0) % 360.0 - 180.0
+    lat = lat0 + (np.arange(H) - 2 + 0.5) * dlat
+    lam, mu = np.radians(lon), np.sin(np.radians(np.clip(lat, -90.0, 90.0)))
+    rng = np.random.default_rng(seed)
+    v = np.zeros((H, W))
+    for _ in range(modes):
+        m, k = int(rng.integers(1, 13)), int(rng.integers(1, 13))
+        a = rng.normal(0.0, 1.0) / math.sqrt(m * m + k * k)
+        p = rng.uniform(0, 2 * math.pi)
+        v += a * np.outer(_legendre(k, mu), np.cos(m * lam + p))
+    inner = v[2:-2, 2:-2]
+    thr = float(np.quantile(inner, 1.0 - land))
+    vmin = float(inner.min())
+    b = np.where(v > thr, land_height, -depth * (thr - v) / (thr - vmin))
+    eta0 = np.zeros((H, W))
+    LON, LAT = np.meshgrid(lon, lat)
+    return {"nx": nx, "ny": ny, "lat0": lat0, "lat1": lat1, "b": b, "eta0": eta0, "lon": LON, "lat": LAT}
