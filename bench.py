@@ -97,9 +97,11 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """Per-launch DRAM bytes of the stage-2 kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_stage2_beach2048.md")
+def profile_traffic(impl):
+    """Per-launch DRAM bytes of stage 2 from the committed ncu summary of the
+    stage kernels in use (the tiled pair, or the fused kernel)."""
+    name = "k_split_stage_beach2048.md" if impl == 1 else "k_stage2_beach2048.md"
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
     with open(path) as f:
@@ -280,15 +282,20 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     st2_bytes = STAGE_BYTES["stage2"] * NX * NY
     achieved = st2_bytes / (avg["stage2"] / 1e3) / 1e9
-    traffic = profile_traffic()
-    roofline = {"bound": "hbm", "kernel": "k_stage<2> (stage 2 + friction + sponge + CFL epilogue)",
+    impl = ctypes.c_int(-1)
+    swe._lib.check(lib.swe_get_stage_kernels(sim._h, ctypes.byref(impl)))
+    traffic = profile_traffic(impl.value)
+    kname = ("k_split_faces + k_split_cells<2> (stage 2: faces, then limiter + gather + update + friction + "
+             "sponge + CFL epilogue)" if impl.value == 1 else
+             "k_stage<2> (stage 2 + friction + sponge + CFL epilogue)")
+    roofline = {"bound": "hbm", "kernel": kname,
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                 "fallback 6.65 TB/s",
                 "traffic": traffic, "algorithmic_bytes_per_launch": st2_bytes,
                 "avg_launch_ms": avg["stage2"],
                 "step_phase_ms": avg,
-                "note": "FP64-issue bound: the kernel's ceiling is the FP64 pipe, not HBM; see DESIGN.md"}
+                "note": "FP64-latency bound stencil: the ceiling is dependent FP64 issue, not HBM"}
 
     # e2e through the C ABI with host buffers: per step upload (h, hu, hv)
     # from pinned host memory, one self-timed step, download (h, hu, hv).

@@ -209,10 +209,12 @@ int swe_vel_batch(swe_sim* s, int n, const double* hq, const double* h, double* 
  * own options, bed, boundaries, Manning n and Flather tide, and its own dt =
  * maxDt() every step) advanced together: one launch per kernel per ensemble
  * step over a tile list of all basins, captured as CUDA graphs.  The
- * schedule (rows per tile, CTAs -- 0 for one CTA per tile, else a persistent
- * grid -- and tile order: 0 basin-major, 1 largest basin first, 2 round
- * robin) is set explicitly or chosen by swe_batch_autotune, which times every
- * candidate on the ensemble itself and restores the state afterwards.  Each
+ * schedule (the stage kernels and their tile: rows per tile 0 for the tiled
+ * pair's 32 x 8 tiles, or 4..64 rows of the fused row-marching tile; CTAs --
+ * 0 for one CTA per tile, else a persistent grid -- and tile order:
+ * 0 basin-major, 1 largest basin first, 2 round robin) is set explicitly or
+ * chosen by swe_batch_autotune, which times every candidate on the ensemble
+ * itself and restores the state afterwards.  Each
  * basin's result is bit-identical to advancing it alone with swe_run.  The
  * reference drives one basin per ShallowWater (src/swe.mjs:145); this is the
  * many-basin form of that loop. */
@@ -274,7 +276,7 @@ int swe_adjoint_get_stream(swe_adjoint* s, void** stream);
  * Two implementations of each SSP-RK2 stage, bit-identical in their results:
  * SWE_STAGE_FUSED, one row-marching kernel per stage that keeps the stencil
  * on chip; SWE_STAGE_SPLIT, two tiled kernels (faces, then cells) that run
- * at higher occupancy through 14 extra fields in device memory (the
+ * at higher occupancy through 12 extra fields in device memory (the
  * default).  The environment variable SWE_B200_STAGE=fused|split overrides
  * the default at creation. */
 #define SWE_STAGE_FUSED 0

@@ -49,7 +49,8 @@ def test_each_basin_matches_single_grid(swe):
 
 
 @pytest.mark.parametrize("sched", [dict(rows=16, ctas=0, order=1), dict(rows=64, ctas=148, order=2),
-                                   dict(rows=24, ctas=37, order=0)])
+                                   dict(rows=24, ctas=37, order=0), dict(rows=0, ctas=0, order=2),
+                                   dict(rows=0, ctas=97, order=1), dict(rows=32, ctas=0, order=0)])
 def test_schedule_does_not_change_results(swe, sched):
     bs = basins(swe)
     ref = swe.Ensemble(bs)
@@ -71,7 +72,7 @@ def test_autotune_keeps_state(swe):
     before = [[ens.field(q, f) for f in ("h", "hu", "hv")] for q in range(len(bs))]
     t_before = [ens.t(q) for q in range(len(bs))]
     res = ens.autotune(trial_steps=2)
-    assert res["rows"] in (16, 24, 32, 48, 64) and res["order"] in (0, 1, 2)
+    assert res["rows"] in (0, 16, 24, 32, 48, 64) and res["order"] in (0, 1, 2)
     for q in range(len(bs)):
         assert ens.t(q) == t_before[q]
         for k, f in enumerate(("h", "hu", "hv")):

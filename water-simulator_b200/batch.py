@@ -2,10 +2,10 @@
 
 Each basin is a full ShallowWater (src/swe.mjs:145 of the reference) with its
 own grid, bed, Manning n, boundaries and Flather tide, stepping with its own
-dt = maxDt().  One ensemble step is five kernel launches over a tile list of
-all basins (swe_batch_* in include/swe_b200.h), captured as CUDA graphs; the
-tile schedule is chosen by `autotune`, which times candidates on the
-ensemble itself and keeps the state unchanged.
+dt = maxDt().  One ensemble step is a handful of kernel launches over a tile
+list of all basins (swe_batch_* in include/swe_b200.h), captured as CUDA
+graphs; the stage kernels and the tile schedule are chosen by `autotune`,
+which times candidates on the ensemble itself and keeps the state unchanged.
 """
 import ctypes
 import json
@@ -108,7 +108,10 @@ class Ensemble:
         check(self._lib.swe_batch_get_schedule(self._h, s))
         return {"rows": s[0], "ctas": s[1], "order": s[2], "tiles": s[3]}
 
-    def set_schedule(self, rows=32, ctas=0, order=0):
+    def set_schedule(self, rows=0, ctas=0, order=0):
+        """rows 0: the tiled stage pair (32 x 8 tiles); 4..64: fused row-marching
+        tiles of that many rows.  ctas 0: one CTA per tile, else a persistent
+        grid.  order 0 basin-major, 1 largest basin first, 2 round robin."""
         check(self._lib.swe_batch_set_schedule(self._h, int(rows), int(ctas), int(order)))
 
     def autotune(self, trial_steps=3, cache=None, key=None):

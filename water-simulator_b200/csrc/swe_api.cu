@@ -270,15 +270,13 @@ int launch_bc(swe_sim* s, double* const* f, int respect_stop) {
 }
 
 // One SSP-RK2 step on the device; `mode`/`dt`/`t_end` as k_prepare.
-// Buffers of the tiled stage kernels (faces and source terms, 14 fields).
+// Buffers of the tiled stage kernels (faces and source terms).
 int ensure_split(swe_sim* s) {
   if (s->d_split) return SWE_OK;
   const size_t N = s->N;
-  CU(cudaMalloc(&s->d_split, sizeof(double) * 14 * N));
-  CU(cudaMemsetAsync(s->d_split, 0, sizeof(double) * 14 * N, s->st));
-  for (int q = 0; q < 5; q++) { s->sb.fx[q] = s->d_split + q * N; s->sb.fy[q] = s->d_split + (5 + q) * N; }
-  for (int q = 0; q < 3; q++) s->sb.tb[q] = s->d_split + (10 + q) * N;
-  s->sb.U = s->d_split + 13 * N;
+  CU(cudaMalloc(&s->d_split, sizeof(double) * swe::SPLIT_FIELDS * N));
+  CU(cudaMemsetAsync(s->d_split, 0, sizeof(double) * swe::SPLIT_FIELDS * N, s->st));
+  s->sb = swe::split_bufs_at(s->d_split, N);
   return SWE_OK;
 }
 

@@ -16,6 +16,7 @@
 // chooses by timing candidates on the ensemble itself.
 #include "../../include/swe_b200.h"
 #include "swe_kernels.cuh"
+#include "swe_split.cuh"
 
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -39,6 +40,7 @@ struct BatchBasin {
   BCArgs bcA, bcB;
   Control* ctl;
   PrepArgs prep;
+  swe::SplitBufs sp;      // faces and source terms of the tiled stage kernels
 };
 
 struct BatchTile { int basin, strip, y0, y1, part; };
@@ -67,6 +69,33 @@ k_batch_stage(BatchBasin* basins, const BatchTile* tiles, int ntiles) {
   }
 }
 
+// The tiled stage pair over the tile list: a tile is (basin, tile column,
+// tile row) of that basin's 32 x 8 tiling; its partial slot closes the
+// basin's step exactly as in the single-grid kernels.
+template <int MODE>
+__global__ void __launch_bounds__(swe::SP_THREADS, 3)
+k_batch_split_faces(BatchBasin* basins, const BatchTile* tiles, int ntiles) {
+  __shared__ swe::FacesSmem sm;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BatchTile tile = tiles[t];
+    const BatchBasin& B = basins[tile.basin];
+    if (!B.ctl->stop) swe::split_faces_tile(MODE == 1 ? B.s1 : B.s2, B.sp, tile.strip, tile.y0, sm);
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(swe::SP_THREADS, SWE_SPLIT_CELLS_MIN_BLOCKS)
+k_batch_split_cells(BatchBasin* basins, const BatchTile* tiles, int ntiles) {
+  __shared__ swe::CellsSmem sm;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BatchTile tile = tiles[t];
+    const BatchBasin& B = basins[tile.basin];
+    const StageArgs& a = MODE == 1 ? B.s1 : B.s2;
+    if (!B.ctl->stop) swe::split_cells_tile<MODE>(a, B.sp, B.ctl, tile.strip, tile.y0, tile.part, a.nblocks, sm);
+    __syncthreads();          // the next tile reuses the shared limiter tile
+  }
+}
+
 int fail(int code, const std::string& m) { swe_host::set_error(m); return code; }
 
 #define CU(call)                                                                      \
@@ -90,6 +119,7 @@ struct swe_batch {
   BatchTile* d_tiles = nullptr;
   int ntiles = 0, tile_cap = 0;
   int rows = 32, ctas = 0, order = 0;   // the schedule
+  int impl = 1;                         // stage kernels: 0 fused tiles, 1 the tiled pair
   int grid = 0;
   double* save = nullptr;           // autotune snapshot of every basin's A and control
   size_t save_doubles = 0;
@@ -102,10 +132,25 @@ namespace {
 
 size_t round_up(size_t n) { return (n + 31) & ~size_t(31); }   // 256-byte multiples
 
+// Partial slots a basin needs: one per tile at the finest tiling either
+// stage implementation uses (4-row fused tiles, or 32 x 8 tiles).
+size_t part_slots(int W, int H) {
+  const size_t fused = (size_t)((W + swe::SX - 1) / swe::SX) * ((H + 3) / 4);
+  const size_t split = (size_t)((W + swe::SPX - 1) / swe::SPX) * ((H + swe::SPY - 1) / swe::SPY);
+  return std::max(fused, split);
+}
+
 // Fill the tile list for the current schedule and upload it.
 int build_tiles(swe_batch* s) {
   std::vector<std::vector<BatchTile>> per(s->nb);
   for (int b = 0; b < s->nb; b++) {
+    if (s->impl == 1) {
+      const int gx = (s->W[b] + swe::SPX - 1) / swe::SPX, gy = (s->H[b] + swe::SPY - 1) / swe::SPY;
+      int part = 0;
+      for (int y = 0; y < gy; y++)
+        for (int x = 0; x < gx; x++) per[b].push_back({b, x, y, 0, part++});
+      continue;
+    }
     const int gx = (s->W[b] + swe::SX - 1) / swe::SX;
     const int gy = (s->H[b] + s->rows - 1) / s->rows;
     const int ry = (s->H[b] + gy - 1) / gy;
@@ -158,11 +203,21 @@ int enqueue_batch_step(swe_batch* s) {
   const dim3 bcg((most + 255) / 256, s->nb);
   k_batch_bc<<<bcg, 256, 0, s->st>>>(s->d_basins, 0);
   CU(cudaGetLastError());
-  k_batch_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+  if (s->impl == 1) {
+    k_batch_split_faces<1><<<s->grid, swe::SP_THREADS, 0, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+    k_batch_split_cells<1><<<s->grid, swe::SP_THREADS, 0, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+  } else {
+    k_batch_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+  }
   CU(cudaGetLastError());
   k_batch_bc<<<bcg, 256, 0, s->st>>>(s->d_basins, 1);
   CU(cudaGetLastError());
-  k_batch_stage<2><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+  if (s->impl == 1) {
+    k_batch_split_faces<2><<<s->grid, swe::SP_THREADS, 0, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+    k_batch_split_cells<2><<<s->grid, swe::SP_THREADS, 0, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+  } else {
+    k_batch_stage<2><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
+  }
   CU(cudaGetLastError());
   return SWE_OK;
 }
@@ -259,9 +314,10 @@ int swe_batch_create(int n, const swe_options* opts, const double* const* b, con
     }
     const size_t N = (size_t)s->W[q] * s->H[q];
     s->off.push_back(total);
-    // b, A (3), B (3), metric rows, partial slots (3 x up to one per tile at 4-row tiles)
-    const size_t parts = (size_t)((s->W[q] + swe::SX - 1) / swe::SX) * ((s->H[q] + 3) / 4);
-    total += round_up(N) * 7 + round_up((size_t)(SWE_GEOM_NROWS + 3) * s->H[q]) + round_up(3 * parts);
+    // b, A (3), B (3), the tiled pair's fields, metric rows, partial slots
+    // (3 x one per tile, for the most tiles either kernel uses)
+    total += round_up(N) * (7 + swe::SPLIT_FIELDS) + round_up((size_t)(SWE_GEOM_NROWS + 3) * s->H[q]) +
+             round_up(3 * part_slots(s->W[q], s->H[q]));
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
@@ -283,10 +339,11 @@ int swe_batch_create(int n, const swe_options* opts, const double* const* b, con
     double* fb = base;
     double* A[3] = {base + rN, base + 2 * rN, base + 3 * rN};
     double* Bf[3] = {base + 4 * rN, base + 5 * rN, base + 6 * rN};
-    double* g = base + 7 * rN;
+    double* spl = base + 7 * rN;                // the tiled pair's fields
+    double* g = base + (7 + swe::SPLIT_FIELDS) * rN;
     const int Hq = s->H[q];
     double* parts = g + round_up((size_t)(SWE_GEOM_NROWS + 3) * Hq);
-    const size_t pcap = (size_t)((s->W[q] + swe::SX - 1) / swe::SX) * ((Hq + 3) / 4);
+    const size_t pcap = part_slots(s->W[q], Hq);
     cudaMemcpyAsync(fb, b[q], sizeof(double) * N, cudaMemcpyHostToDevice, s->st);
     cudaMemcpyAsync(A[0], h[q], sizeof(double) * N, cudaMemcpyHostToDevice, s->st);
     cudaMemcpyAsync(g, geom[q].data(), sizeof(double) * geom[q].size(), cudaMemcpyHostToDevice, s->st);
@@ -322,6 +379,7 @@ int swe_batch_create(int n, const swe_options* opts, const double* const* b, con
     B.bcA = bc; B.bcA.h = A[0]; B.bcA.hu = A[1]; B.bcA.hv = A[2];
     B.bcB = bc; B.bcB.h = Bf[0]; B.bcB.hu = Bf[1]; B.bcB.hv = Bf[2];
     B.ctl = s->ctls + q;
+    B.sp = swe::split_bufs_at(spl, rN);
     B.prep.mode = 1; B.prep.dt_host = 0; B.prep.cfl = o.cfl; B.prep.t_end = INFINITY;
   }
   int rc = build_tiles(s);
@@ -374,15 +432,18 @@ int swe_batch_set_flather_tide(swe_batch* s, int basin, int side, double msl, in
 }
 
 int swe_batch_set_schedule(swe_batch* s, int rows_per_tile, int ctas, int order) {
-  if (!s || rows_per_tile < 4 || rows_per_tile > swe::RY_MAX || ctas < 0 || order < 0 || order > 2)
-    return fail(SWE_EINVAL, "swe_batch_set_schedule: rows in [4, 64], ctas >= 0, order 0..2");
-  s->rows = rows_per_tile; s->ctas = ctas; s->order = order;
+  if (!s || !(rows_per_tile == 0 || (rows_per_tile >= 4 && rows_per_tile <= swe::RY_MAX)) || ctas < 0 ||
+      order < 0 || order > 2)
+    return fail(SWE_EINVAL, "swe_batch_set_schedule: rows 0 (tiled pair) or in [4, 64], ctas >= 0, order 0..2");
+  s->impl = rows_per_tile == 0 ? 1 : 0;
+  if (rows_per_tile) s->rows = rows_per_tile;
+  s->ctas = ctas; s->order = order;
   return build_tiles(s);
 }
 
 int swe_batch_get_schedule(swe_batch* s, int* out4) {
   if (!s || !out4) return fail(SWE_EINVAL, "null argument");
-  out4[0] = s->rows; out4[1] = s->ctas; out4[2] = s->order; out4[3] = s->ntiles;
+  out4[0] = s->impl == 1 ? 0 : s->rows; out4[1] = s->ctas; out4[2] = s->order; out4[3] = s->ntiles;
   return SWE_OK;
 }
 
@@ -454,21 +515,25 @@ int swe_batch_autotune(swe_batch* s, int trial_steps, int* best4, double* best_m
   };
   int rc = snapshot(false);
   if (rc) return rc;
-  int dev = 0, sms = 148, occ = 3;
+  int dev = 0, sms = 148, occ = 3, occ_split = 3;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_stage<2>, swe::BX, swe::STAGE_SMEM_BYTES);
-  const int rows_c[] = {16, 24, 32, 48, 64};
-  const int ctas_c[] = {0, sms * std::max(occ, 1), 2 * sms * std::max(occ, 1)};
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_split, k_batch_split_faces<2>, swe::SP_THREADS, 0);
+  const int rows_c[] = {0, 16, 24, 32, 48, 64};          // 0: the tiled pair
   double best = INFINITY;
-  int br = s->rows, bc = s->ctas, bo = s->order;
+  int bi = s->impl, br = s->rows, bc = s->ctas, bo = s->order;
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
   for (int r : rows_c)
-    for (int c : ctas_c)
+    for (int ci = 0; ci < 3; ci++)
       for (int o = 0; o < 3; o++) {
-        s->rows = r; s->ctas = c; s->order = o;
+        const int per_sm = std::max(r == 0 ? occ_split : occ, 1);
+        const int c = ci == 0 ? 0 : ci * sms * per_sm;
+        s->impl = r == 0 ? 1 : 0;
+        if (r) s->rows = r;
+        s->ctas = c; s->order = o;
         rc = build_tiles(s);
         if (rc) return rc;
         rc = run_steps(s, 1);                    // warm
@@ -480,17 +545,17 @@ int swe_batch_autotune(swe_batch* s, int trial_steps, int* best4, double* best_m
         CU(cudaEventSynchronize(e1));
         float ms = 0;
         CU(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) { best = ms; br = r; bc = c; bo = o; }
+        if (ms < best) { best = ms; bi = s->impl; br = s->rows; bc = c; bo = o; }
         rc = snapshot(true);
         if (rc) return rc;
       }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  s->rows = br; s->ctas = bc; s->order = bo;
+  s->impl = bi; s->rows = br; s->ctas = bc; s->order = bo;
   rc = build_tiles(s);
   if (rc) return rc;
   CU(cudaStreamSynchronize(s->st));
-  if (best4) { best4[0] = br; best4[1] = bc; best4[2] = bo; best4[3] = s->ntiles; }
+  if (best4) { best4[0] = bi == 1 ? 0 : br; best4[1] = bc; best4[2] = bo; best4[3] = s->ntiles; }
   if (best_ms) *best_ms = best / trial_steps;
   return SWE_OK;
 }

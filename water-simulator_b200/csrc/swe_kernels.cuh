@@ -94,6 +94,10 @@ struct StageArgs {
   int sponge_side, sponge_width; const double* sponge_str; double sponge_ref;
   double* part_max; double* part_fl1; double* part_fl2;     // one per CTA
   int nblocks;
+  // optional tape of the tiled stage kernels (the adjoint's segment pass):
+  // the cell's positivity limiter, its depth before dryClean and (stage 2)
+  // the state after dryClean that friction takes
+  double* tape_th; double* tape_hpre; double* tape_pre[3];
 };
 
 // ---------------------------------------------------------------------------

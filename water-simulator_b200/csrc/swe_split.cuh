@@ -20,8 +20,11 @@
 //                   sponge, CFL rate; src/swe.mjs:659-813).  The last block
 //                   to finish closes the step as the fused kernel does.
 //
-// Face arrays are indexed by their left / lower cell and are zero where no
-// face exists, so the limiter reads them unconditionally.
+// Both are written as tile functions (split_faces_tile, split_cells_tile)
+// that a single-grid kernel calls once and the batched ensemble calls for
+// every tile of its tile list.  Face arrays are indexed by their left /
+// lower cell and are zero where no face exists, so the limiter reads them
+// unconditionally.
 #pragma once
 
 #include "swe_kernels.cuh"
@@ -33,96 +36,48 @@ constexpr int SPX = 32, SPY = 8;                 // tile of owned cells
 constexpr int SP_THREADS = SPX * SPY;
 constexpr int SSX = SPX + 3, SSY = SPY + 3;     // state tile: cols i0-1 .. i0+SPX+1, rows j0-1 .. j0+SPY+1
 
+// A face is kept as the four values the gather reads: the mass flux M, the
+// transverse flux T, and the normal-momentum flux plus each side's pressure
+// correction, N + pL for the left / lower cell and N + pR for the right /
+// upper one (the same sums the gather forms, so no rounding changes).
+enum { F_M = 0, F_T = 1, F_NPL = 2, F_NPR = 3, SPLIT_FACE_FIELDS = 4 };
+constexpr int SPLIT_FIELDS = 2 * SPLIT_FACE_FIELDS + 4;   // faces, 3 source terms, u
+
 struct SplitBufs {
-  double* fx[5];        // x face (k|k+1): M N T pL pR
-  double* fy[5];        // y face (k|k+W)
-  double* tb[3];        // bed term x, bed term y, geometric source
-  double* U;            // cell velocity u (spherical Coriolis)
+  double* fx[SPLIT_FACE_FIELDS];   // x face (k|k+1)
+  double* fy[SPLIT_FACE_FIELDS];   // y face (k|k+W)
+  double* tb[3];                   // bed term x, bed term y, geometric source
+  double* U;                       // cell velocity u (spherical Coriolis)
 };
 
-__global__ void __launch_bounds__(SP_THREADS, 3) k_split_faces(StageArgs a, SplitBufs s, Control* ctl) {
-  if (ctl->stop) return;
-  __shared__ double s_b[SSY][SSX], s_h[SSY][SSX], s_U[SSY][SSX], s_V[SSY][SSX];
-  __shared__ double s_xs[4][SPY][SPX + 1];      // x slopes of cols i0 .. i0+SPX, rows j0 .. j0+SPY-1
-  __shared__ double s_ys[4][SPY + 1][SPX];      // y slopes of cols i0 .. i0+SPX-1, rows j0 .. j0+SPY
+// The SPLIT_FIELDS fields of one grid, `stride` doubles apart from `base`.
+__host__ __forceinline__ SplitBufs split_bufs_at(double* base, size_t stride) {
+  SplitBufs b;
+  for (int q = 0; q < SPLIT_FACE_FIELDS; q++) {
+    b.fx[q] = base + q * stride;
+    b.fy[q] = base + (SPLIT_FACE_FIELDS + q) * stride;
+  }
+  for (int q = 0; q < 3; q++) b.tb[q] = base + (2 * SPLIT_FACE_FIELDS + q) * stride;
+  b.U = base + (2 * SPLIT_FACE_FIELDS + 3) * stride;
+  return b;
+}
+
+struct FacesSmem {
+  double b[SSY][SSX], h[SSY][SSX], U[SSY][SSX], V[SSY][SSX];
+  double xs[4][SPY][SPX + 1];                   // x slopes of cols i0 .. i0+SPX, rows j0 .. j0+SPY-1
+  double ys[4][SPY + 1][SPX];                   // y slopes of cols i0 .. i0+SPX-1, rows j0 .. j0+SPY
+};
+
+// One cell of a faces tile: its source terms, its east x face and north y face.
+__device__ __forceinline__ void split_faces_cell(const StageArgs& a, const SplitBufs& s, const FacesSmem& sm,
+                                                 int lx, int ly, int gi, int gj, bool sph, bool bedOn) {
   const int W = a.W, H = a.H;
-  const int i0 = blockIdx.x * SPX, j0 = blockIdx.y * SPY;
-  const double dry = a.minDepth, eps4 = a.eps4;
-  const bool order2 = a.order >= 2;
-  const bool sph = a.sph != 0;
-  const bool bedOn = order2 || sph;
-  const int t = threadIdx.x;
-
-  // state and velocities of the tile and its halo (zero outside the grid)
-  for (int q = t; q < SSX * SSY; q += SP_THREADS) {
-    const int ly = q / SSX, lx = q - ly * SSX;
-    const int gi = i0 - 1 + lx, gj = j0 - 1 + ly;
-    double b = 0, h = 0, U = 0, V = 0;
-    if (gi >= 0 && gi < W && gj >= 0 && gj < H) {
-      const int k = gj * W + gi;
-      b = __ldg(a.b + k); h = __ldg(a.h + k);
-      const double hu = __ldg(a.hu + k), hv = __ldg(a.hv + k);
-      if (h == 0) {                  // +-0 / den == +-0 and NaN / den == NaN: no division needed
-        U = vel_num(hu, h); V = vel_num(hv, h);
-      } else {
-        const double den = vel_den(h, eps4);
-        U = vel_num(hu, h) / den; V = vel_num(hv, h) / den;
-      }
-    }
-    s_b[ly][lx] = b; s_h[ly][lx] = h; s_U[ly][lx] = U; s_V[ly][lx] = V;
-  }
-  __syncthreads();
-
-  // x slopes (src/swe.mjs:364-411, d = 0)
-  for (int q = t; q < SPY * (SPX + 1); q += SP_THREADS) {
-    const int ly = q / (SPX + 1), lx = q - ly * (SPX + 1);
-    const int gi = i0 + lx, gj = j0 + ly;
-    double sE = 0, sB = 0, sU = 0, sV = 0;
-    if (order2 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1) {
-      const int cy = ly + 1, cx = lx + 1;
-      const double hk = s_h[cy][cx], hp = s_h[cy][cx + 1], hm = s_h[cy][cx - 1];
-      if (!(hk <= dry || hp <= dry || hm <= dry)) {
-        const double bk = s_b[cy][cx], bp = s_b[cy][cx + 1], bm = s_b[cy][cx - 1];
-        const double eC = bk + hk, eP = bp + hp, eM = bm + hm;
-        const double uk = s_U[cy][cx], vk = s_V[cy][cx];
-        sE = limiter(a.lim, eC - eM, eP - eC);
-        sB = limiter(a.lim, bk - bm, bp - bk);
-        sU = limiter(a.lim, uk - s_U[cy][cx - 1], s_U[cy][cx + 1] - uk);
-        sV = limiter(a.lim, vk - s_V[cy][cx - 1], s_V[cy][cx + 1] - vk);
-      }
-    }
-    s_xs[0][ly][lx] = sE; s_xs[1][ly][lx] = sB; s_xs[2][ly][lx] = sU; s_xs[3][ly][lx] = sV;
-  }
-  // y slopes (d = 1)
-  for (int q = t; q < (SPY + 1) * SPX; q += SP_THREADS) {
-    const int ly = q / SPX, lx = q - ly * SPX;
-    const int gi = i0 + lx, gj = j0 + ly;
-    double sE = 0, sB = 0, sU = 0, sV = 0;
-    if (order2 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1) {
-      const int cy = ly + 1, cx = lx + 1;
-      const double hk = s_h[cy][cx], hp = s_h[cy + 1][cx], hm = s_h[cy - 1][cx];
-      if (!(hk <= dry || hp <= dry || hm <= dry)) {
-        const double bk = s_b[cy][cx], bp = s_b[cy + 1][cx], bm = s_b[cy - 1][cx];
-        const double eC = bk + hk, eP = bp + hp, eM = bm + hm;
-        const double uk = s_U[cy][cx], vk = s_V[cy][cx];
-        sE = limiter(a.lim, eC - eM, eP - eC);
-        sB = limiter(a.lim, bk - bm, bp - bk);
-        sU = limiter(a.lim, uk - s_U[cy - 1][cx], s_U[cy + 1][cx] - uk);
-        sV = limiter(a.lim, vk - s_V[cy - 1][cx], s_V[cy + 1][cx] - vk);
-      }
-    }
-    s_ys[0][ly][lx] = sE; s_ys[1][ly][lx] = sB; s_ys[2][ly][lx] = sU; s_ys[3][ly][lx] = sV;
-  }
-  __syncthreads();
-
-  const int lx = t % SPX, ly = t / SPX;
-  const int gi = i0 + lx, gj = j0 + ly;
-  if (gi >= W || gj >= H) return;
+  const double dry = a.minDepth;
   const int k = gj * W + gi;
   const int cx = lx + 1, cy = ly + 1;
-  const double bk = s_b[cy][cx], hk = s_h[cy][cx], Uk = s_U[cy][cx], Vk = s_V[cy][cx];
-  const double xsE = s_xs[0][ly][lx], xsB = s_xs[1][ly][lx];
-  const double nsE = s_ys[0][ly][lx], nsB = s_ys[1][ly][lx];
+  const double bk = sm.b[cy][cx], hk = sm.h[cy][cx], Uk = sm.U[cy][cx], Vk = sm.V[cy][cx];
+  const double xsE = sm.xs[0][ly][lx], xsB = sm.xs[1][ly][lx];
+  const double nsE = sm.ys[0][ly][lx], nsB = sm.ys[1][ly][lx];
 
   // bed term and geometric source of the cell (src/swe.mjs:570-598)
   double tb0 = 0, tb1 = 0, tg = 0;
@@ -146,19 +101,105 @@ __global__ void __launch_bounds__(SP_THREADS, 3) k_split_faces(StageArgs a, Spli
   // east x face (k|k+1)
   Face fx = {0, 0, 0, 0, 0};
   if (gj >= 2 && gj < H - 2 && gi >= 1 && gi < W - 2) {
-    fx = face_flux(bk, hk, Uk, Vk, xsE, xsB, s_xs[2][ly][lx], s_xs[3][ly][lx],
-                   s_b[cy][cx + 1], s_h[cy][cx + 1], s_U[cy][cx + 1], s_V[cy][cx + 1],
-                   s_xs[0][ly][lx + 1], s_xs[1][ly][lx + 1], s_xs[2][ly][lx + 1], s_xs[3][ly][lx + 1], dry);
+    fx = face_flux(bk, hk, Uk, Vk, xsE, xsB, sm.xs[2][ly][lx], sm.xs[3][ly][lx],
+                   sm.b[cy][cx + 1], sm.h[cy][cx + 1], sm.U[cy][cx + 1], sm.V[cy][cx + 1],
+                   sm.xs[0][ly][lx + 1], sm.xs[1][ly][lx + 1], sm.xs[2][ly][lx + 1], sm.xs[3][ly][lx + 1], dry);
   }
-  s.fx[0][k] = fx.M; s.fx[1][k] = fx.N; s.fx[2][k] = fx.T; s.fx[3][k] = fx.pL; s.fx[4][k] = fx.pR;
+  s.fx[F_M][k] = fx.M; s.fx[F_T][k] = fx.T; s.fx[F_NPL][k] = fx.N + fx.pL; s.fx[F_NPR][k] = fx.N + fx.pR;
   // north y face (k|k+W): v is normal, u transverse
   Face fy = {0, 0, 0, 0, 0};
   if (gj >= 1 && gj < H - 2 && gi >= 2 && gi < W - 2) {
-    fy = face_flux(bk, hk, Vk, Uk, nsE, nsB, s_ys[3][ly][lx], s_ys[2][ly][lx],
-                   s_b[cy + 1][cx], s_h[cy + 1][cx], s_V[cy + 1][cx], s_U[cy + 1][cx],
-                   s_ys[0][ly + 1][lx], s_ys[1][ly + 1][lx], s_ys[3][ly + 1][lx], s_ys[2][ly + 1][lx], dry);
+    fy = face_flux(bk, hk, Vk, Uk, nsE, nsB, sm.ys[3][ly][lx], sm.ys[2][ly][lx],
+                   sm.b[cy + 1][cx], sm.h[cy + 1][cx], sm.V[cy + 1][cx], sm.U[cy + 1][cx],
+                   sm.ys[0][ly + 1][lx], sm.ys[1][ly + 1][lx], sm.ys[3][ly + 1][lx], sm.ys[2][ly + 1][lx], dry);
   }
-  s.fy[0][k] = fy.M; s.fy[1][k] = fy.N; s.fy[2][k] = fy.T; s.fy[3][k] = fy.pL; s.fy[4][k] = fy.pR;
+  s.fy[F_M][k] = fy.M; s.fy[F_T][k] = fy.T; s.fy[F_NPL][k] = fy.N + fy.pL; s.fy[F_NPR][k] = fy.N + fy.pR;
+}
+
+// Faces and source terms of the tile (tx, ty).  Every thread of the CTA
+// calls it; it returns with the shared memory free for the next tile.
+__device__ __forceinline__ void split_faces_tile(const StageArgs& a, const SplitBufs& s, int tx, int ty,
+                                                 FacesSmem& sm) {
+  const int W = a.W, H = a.H;
+  const int i0 = tx * SPX, j0 = ty * SPY;
+  const double dry = a.minDepth, eps4 = a.eps4;
+  const bool order2 = a.order >= 2;
+  const bool sph = a.sph != 0;
+  const bool bedOn = order2 || sph;
+  const int t = threadIdx.x;
+
+  // state and velocities of the tile and its halo (zero outside the grid)
+  for (int q = t; q < SSX * SSY; q += SP_THREADS) {
+    const int ly = q / SSX, lx = q - ly * SSX;
+    const int gi = i0 - 1 + lx, gj = j0 - 1 + ly;
+    double b = 0, h = 0, U = 0, V = 0;
+    if (gi >= 0 && gi < W && gj >= 0 && gj < H) {
+      const int k = gj * W + gi;
+      b = __ldg(a.b + k); h = __ldg(a.h + k);
+      const double hu = __ldg(a.hu + k), hv = __ldg(a.hv + k);
+      if (h == 0) {                  // +-0 / den == +-0 and NaN / den == NaN: no division needed
+        U = vel_num(hu, h); V = vel_num(hv, h);
+      } else {
+        const double den = vel_den(h, eps4);
+        U = vel_num(hu, h) / den; V = vel_num(hv, h) / den;
+      }
+    }
+    sm.b[ly][lx] = b; sm.h[ly][lx] = h; sm.U[ly][lx] = U; sm.V[ly][lx] = V;
+  }
+  __syncthreads();
+
+  // x slopes (src/swe.mjs:364-411, d = 0)
+  for (int q = t; q < SPY * (SPX + 1); q += SP_THREADS) {
+    const int ly = q / (SPX + 1), lx = q - ly * (SPX + 1);
+    const int gi = i0 + lx, gj = j0 + ly;
+    double sE = 0, sB = 0, sU = 0, sV = 0;
+    if (order2 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1) {
+      const int cy = ly + 1, cx = lx + 1;
+      const double hk = sm.h[cy][cx], hp = sm.h[cy][cx + 1], hm = sm.h[cy][cx - 1];
+      if (!(hk <= dry || hp <= dry || hm <= dry)) {
+        const double bk = sm.b[cy][cx], bp = sm.b[cy][cx + 1], bm = sm.b[cy][cx - 1];
+        const double eC = bk + hk, eP = bp + hp, eM = bm + hm;
+        const double uk = sm.U[cy][cx], vk = sm.V[cy][cx];
+        sE = limiter(a.lim, eC - eM, eP - eC);
+        sB = limiter(a.lim, bk - bm, bp - bk);
+        sU = limiter(a.lim, uk - sm.U[cy][cx - 1], sm.U[cy][cx + 1] - uk);
+        sV = limiter(a.lim, vk - sm.V[cy][cx - 1], sm.V[cy][cx + 1] - vk);
+      }
+    }
+    sm.xs[0][ly][lx] = sE; sm.xs[1][ly][lx] = sB; sm.xs[2][ly][lx] = sU; sm.xs[3][ly][lx] = sV;
+  }
+  // y slopes (d = 1)
+  for (int q = t; q < (SPY + 1) * SPX; q += SP_THREADS) {
+    const int ly = q / SPX, lx = q - ly * SPX;
+    const int gi = i0 + lx, gj = j0 + ly;
+    double sE = 0, sB = 0, sU = 0, sV = 0;
+    if (order2 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1) {
+      const int cy = ly + 1, cx = lx + 1;
+      const double hk = sm.h[cy][cx], hp = sm.h[cy + 1][cx], hm = sm.h[cy - 1][cx];
+      if (!(hk <= dry || hp <= dry || hm <= dry)) {
+        const double bk = sm.b[cy][cx], bp = sm.b[cy + 1][cx], bm = sm.b[cy - 1][cx];
+        const double eC = bk + hk, eP = bp + hp, eM = bm + hm;
+        const double uk = sm.U[cy][cx], vk = sm.V[cy][cx];
+        sE = limiter(a.lim, eC - eM, eP - eC);
+        sB = limiter(a.lim, bk - bm, bp - bk);
+        sU = limiter(a.lim, uk - sm.U[cy - 1][cx], sm.U[cy + 1][cx] - uk);
+        sV = limiter(a.lim, vk - sm.V[cy - 1][cx], sm.V[cy + 1][cx] - vk);
+      }
+    }
+    sm.ys[0][ly][lx] = sE; sm.ys[1][ly][lx] = sB; sm.ys[2][ly][lx] = sU; sm.ys[3][ly][lx] = sV;
+  }
+  __syncthreads();
+
+  const int lx = t % SPX, ly = t / SPX;
+  const int gi = i0 + lx, gj = j0 + ly;
+  if (gi < W && gj < H) split_faces_cell(a, s, sm, lx, ly, gi, gj, sph, bedOn);
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(SP_THREADS, 3) k_split_faces(StageArgs a, SplitBufs s, Control* ctl) {
+  if (ctl->stop) return;
+  __shared__ FacesSmem sm;
+  split_faces_tile(a, s, blockIdx.x, blockIdx.y, sm);
 }
 
 // Positivity limiter of cell (gi, gj) from its four faces' mass fluxes
@@ -167,8 +208,8 @@ __device__ __forceinline__ double split_theta(const StageArgs& a, const SplitBuf
   const int W = a.W, H = a.H;
   if (!(dt > 0 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1)) return 1;
   const int k = gj * W + gi;
-  const double fxE = s.fx[0][k], fxW = s.fx[0][k - 1];
-  const double fyN = s.fy[0][k], fyS = s.fy[0][k - W];
+  const double fxE = s.fx[F_M][k], fxW = s.fx[F_M][k - 1];
+  const double fyN = s.fy[F_M][k], fyS = s.fy[F_M][k - W];
   const double avail = a.h[k];
   const double est = ((fxE > 0 ? fxE : 0) - (fxW < 0 ? fxW : 0)) * a.m.rdxRow[gj]
                    + (fyN > 0 ? fyN : 0) * a.m.rdyRowN[gj] - (fyS < 0 ? fyS : 0) * a.m.rdyRowS[gj];
@@ -184,15 +225,21 @@ __device__ __forceinline__ double split_theta(const StageArgs& a, const SplitBuf
   return th;
 }
 
+struct CellsSmem {
+  double th[SPY + 2][SPX + 2];
+  double red[2][SP_THREADS / 32];
+  bool last;
+};
+
+// Limiter, gather, update and epilogue of the tile (tx, ty), which holds
+// partial slot `part` of the `nparts` of its grid; the last tile of the
+// grid to finish closes the step.  Every thread of the CTA calls it.
 template <int MODE>
-__global__ void __launch_bounds__(SP_THREADS) k_split_cells(StageArgs a, SplitBufs s, Control* ctl) {
+__device__ __forceinline__ void split_cells_tile(const StageArgs& a, const SplitBufs& s, Control* ctl, int tx,
+                                                 int ty, int part, int nparts, CellsSmem& sm) {
   static_assert(MODE == 1 || MODE == 2, "stages only");
-  if (ctl->stop) return;
-  __shared__ double s_th[SPY + 2][SPX + 2];
-  __shared__ double s_red[2][SP_THREADS / 32];
-  __shared__ bool s_last;
   const int W = a.W, H = a.H;
-  const int i0 = blockIdx.x * SPX, j0 = blockIdx.y * SPY;
+  const int i0 = tx * SPX, j0 = ty * SPY;
   const int t = threadIdx.x;
   const double dt = ctl->dt;
   const double dry = a.minDepth, eps4 = a.eps4;
@@ -203,7 +250,7 @@ __global__ void __launch_bounds__(SP_THREADS) k_split_cells(StageArgs a, SplitBu
 
   for (int q = t; q < (SPX + 2) * (SPY + 2); q += SP_THREADS) {
     const int ly = q / (SPX + 2), lx = q - ly * (SPX + 2);
-    s_th[ly][lx] = split_theta(a, s, dt, i0 - 1 + lx, j0 - 1 + ly);
+    sm.th[ly][lx] = split_theta(a, s, dt, i0 - 1 + lx, j0 - 1 + ly);
   }
   __syncthreads();
 
@@ -212,48 +259,53 @@ __global__ void __launch_bounds__(SP_THREADS) k_split_cells(StageArgs a, SplitBu
   const int gi = i0 + lx, gj = j0 + ly;
   if (gi < W && gj < H) {
     const int k = gj * W + gi;
-    const double thC = s_th[ly + 1][lx + 1];
+    // every load of the cell first, so they are in flight together
+    const bool rowX = gj >= 2 && gj < H - 2, colY = gi >= 2 && gi < W - 2;
+    const bool hasW = rowX && gi - 1 >= 1 && gi - 1 < W - 2, hasE = rowX && gi >= 1 && gi < W - 2;
+    const bool hasS = colY && gj - 1 >= 1 && gj - 1 < H - 2, hasN = colY && gj >= 1 && gj < H - 2;
+    const bool interior = colY && rowX;
+    double wM = 0, wT = 0, wN = 0, eM = 0, eT = 0, eN = 0, sM = 0, sT = 0, sN = 0, nM = 0, nT = 0, nN = 0;
+    if (hasW) { wM = s.fx[F_M][k - 1]; wT = s.fx[F_T][k - 1]; wN = s.fx[F_NPR][k - 1]; }
+    if (hasE) { eM = s.fx[F_M][k]; eT = s.fx[F_T][k]; eN = s.fx[F_NPL][k]; }
+    if (hasS) { sM = s.fy[F_M][k - W]; sT = s.fy[F_T][k - W]; sN = s.fy[F_NPR][k - W]; }
+    if (hasN) { nM = s.fy[F_M][k]; nT = s.fy[F_T][k]; nN = s.fy[F_NPL][k]; }
+    const double hin = a.h[k], huin = a.hu[k], hvin = a.hv[k];
+    double tb0 = 0, tb1 = 0, tg = 0, Uk = 0;
+    if (interior && bedOn) { tb0 = s.tb[0][k]; tb1 = s.tb[1][k]; if (sph) tg = s.tb[2][k]; }
+    if (interior && sph) Uk = s.U[k];
+    double U0h = 0, U0hu = 0, U0hv = 0;
+    if (MODE == 2) { U0h = a.oh[k]; U0hu = a.ohu[k]; U0hv = a.ohv[k]; }
+    const double thC = sm.th[ly + 1][lx + 1];
     const double rdx = a.m.rdxRow[gj], dxr = a.m.dxRow[gj];
     double ah = 0, ahu = 0, ahv = 0;
-    if (gj >= 2 && gj < H - 2) {
-      if (gi - 1 >= 1 && gi - 1 < W - 2) {            // west face, cell is its right side
-        const double M = s.fx[0][k - 1];
-        const double thf = M >= 0 ? s_th[ly + 1][lx] : thC;
-        const double inv = thf == 1 ? rdx : thf / dxr;
-        ah += M * inv; ahu += (s.fx[1][k - 1] + s.fx[4][k - 1]) * inv; ahv += s.fx[2][k - 1] * inv;
-      }
-      if (gi >= 1 && gi < W - 2) {                    // east face, cell is its left side
-        const double M = s.fx[0][k];
-        const double thf = M >= 0 ? thC : s_th[ly + 1][lx + 2];
-        const double inv = thf == 1 ? rdx : thf / dxr;
-        ah -= M * inv; ahu -= (s.fx[1][k] + s.fx[3][k]) * inv; ahv -= s.fx[2][k] * inv;
-      }
+    if (hasW) {                                       // west face, cell is its right side
+      const double thf = wM >= 0 ? sm.th[ly + 1][lx] : thC;
+      const double inv = thf == 1 ? rdx : thf / dxr;
+      ah += wM * inv; ahu += wN * inv; ahv += wT * inv;
     }
-    if (gi >= 2 && gi < W - 2) {
-      if (gj - 1 >= 1 && gj - 1 < H - 2) {            // south face, cell is its upper side
-        const int kf = k - W;
-        const double M = s.fy[0][kf];
-        const double thf = M >= 0 ? s_th[ly][lx + 1] : thC;
-        const double invR = thf == 1 ? a.m.rdyRowS[gj] : thf / a.m.dyRowS[gj];
-        ah += M * invR; ahv += (s.fy[1][kf] + s.fy[4][kf]) * invR; ahu += s.fy[2][kf] * invR;
-      }
-      if (gj >= 1 && gj < H - 2) {                    // north face, cell is its lower side
-        const double M = s.fy[0][k];
-        const double thf = M >= 0 ? thC : s_th[ly + 2][lx + 1];
-        const double invL = thf == 1 ? a.m.rdyRowN[gj] : thf / a.m.dyRowN[gj];
-        ah -= M * invL; ahv -= (s.fy[1][k] + s.fy[3][k]) * invL; ahu -= s.fy[2][k] * invL;
-      }
+    if (hasE) {                                       // east face, cell is its left side
+      const double thf = eM >= 0 ? thC : sm.th[ly + 1][lx + 2];
+      const double inv = thf == 1 ? rdx : thf / dxr;
+      ah -= eM * inv; ahu -= eN * inv; ahv -= eT * inv;
     }
-    const bool interior = gi >= 2 && gi < W - 2 && gj >= 2 && gj < H - 2;
-    const double hin = a.h[k], huin = a.hu[k], hvin = a.hv[k];
+    if (hasS) {                                       // south face, cell is its upper side
+      const double thf = sM >= 0 ? sm.th[ly][lx + 1] : thC;
+      const double invR = thf == 1 ? a.m.rdyRowS[gj] : thf / a.m.dyRowS[gj];
+      ah += sM * invR; ahv += sN * invR; ahu += sT * invR;
+    }
+    if (hasN) {                                       // north face, cell is its lower side
+      const double thf = nM >= 0 ? thC : sm.th[ly + 2][lx + 1];
+      const double invL = thf == 1 ? a.m.rdyRowN[gj] : thf / a.m.dyRowN[gj];
+      ah -= nM * invL; ahv -= nN * invL; ahu -= nT * invL;
+    }
     if (interior) {
       if (bedOn) {
-        ahu += s.tb[0][k];
-        ahv += s.tb[1][k];
-        if (sph) ahv += s.tb[2][k];
+        ahu += tb0;
+        ahv += tb1;
+        if (sph) ahv += tg;
       }
       if (sph) {
-        const double fe = a.m.fRow[gj] + s.U[k] * (a.m.tanPhi[gj] / a.m.R);
+        const double fe = a.m.fRow[gj] + Uk * (a.m.tanPhi[gj] / a.m.R);
         ahu += fe * hvin;
         ahv -= fe * huin;
       } else if (corOn) {
@@ -261,22 +313,26 @@ __global__ void __launch_bounds__(SP_THREADS) k_split_cells(StageArgs a, SplitBu
         ahv -= a.coriolis * huin;
       }
     }
+    if (a.tape_th) a.tape_th[k] = thC;
     if (MODE == 1) {
       double nh = hin + dt * ah, nhu = huin + dt * ahu, nhv = hvin + dt * ahv;
+      if (a.tape_hpre) a.tape_hpre[k] = nh;
       if (interior) {                                 // dryClean, src/swe.mjs:734-745
         if (nh < 0) { locFl -= nh; nh = 0; }
         if (nh <= dry) { nhu = 0; nhv = 0; }
       }
       a.oh[k] = nh; a.ohu[k] = nhu; a.ohv[k] = nhv;
     } else {
-      const double h0 = a.oh[k], hu0 = a.ohu[k], hv0 = a.ohv[k];   // U0 (in place)
+      const double h0 = U0h, hu0 = U0hu, hv0 = U0hv;   // U0 (in place)
       if (a.h0c) { a.h0c[k] = h0; a.hu0c[k] = hu0; a.hv0c[k] = hv0; }
       double nh = 0.5 * (h0 + hin + dt * ah);
       double nhu = 0.5 * (hu0 + huin + dt * ahu);
       double nhv = 0.5 * (hv0 + hvin + dt * ahv);
+      if (a.tape_hpre) a.tape_hpre[k] = nh;
       if (interior) {
         if (nh < 0) { locFl -= nh; nh = 0; }
         if (nh <= dry) { nhu = 0; nhv = 0; }
+        if (a.tape_pre[0]) { a.tape_pre[0][k] = nh; a.tape_pre[1][k] = nhu; a.tape_pre[2][k] = nhv; }
         // friction, src/swe.mjs:659-704
         const double n = a.nfield ? a.nfield[k] : a.manning;
         const bool fricOn = a.nfield ? true : (n != 0 && n == n);
@@ -320,32 +376,30 @@ __global__ void __launch_bounds__(SP_THREADS) k_split_cells(StageArgs a, SplitBu
     }
   }
 
-  // per-block partials, then the last block closes the step
+  // per-block partials, then the last block of the grid closes the step
   for (int o = 16; o > 0; o >>= 1) {
     locMax = fmax(locMax, __shfl_down_sync(0xffffffffu, locMax, o));
     locFl += __shfl_down_sync(0xffffffffu, locFl, o);
   }
-  if ((t & 31) == 0) { s_red[0][t >> 5] = locMax; s_red[1][t >> 5] = locFl; }
+  if ((t & 31) == 0) { sm.red[0][t >> 5] = locMax; sm.red[1][t >> 5] = locFl; }
   __syncthreads();
-  const int bid = blockIdx.y * gridDim.x + blockIdx.x;
-  const int nb = gridDim.x * gridDim.y;
   if (t == 0) {
-    double m = s_red[0][0], f = s_red[1][0];
-    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, s_red[0][w]); f += s_red[1][w]; }
-    if (MODE == 1) a.part_fl1[bid] = f;
-    else { a.part_max[bid] = m; a.part_fl2[bid] = f; }
+    double m = sm.red[0][0], f = sm.red[1][0];
+    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, sm.red[0][w]); f += sm.red[1][w]; }
+    if (MODE == 1) a.part_fl1[part] = f;
+    else { a.part_max[part] = m; a.part_fl2[part] = f; }
     __threadfence();
     const unsigned int ticket = atomicAdd(&ctl->counter, 1u);
-    s_last = (ticket == (unsigned int)(nb - 1));
+    sm.last = (ticket == (unsigned int)(nparts - 1));
   }
   __syncthreads();
-  if (!s_last) return;
+  if (!sm.last) return;                         // uniform across the CTA
   __threadfence();
   // the whole last block reduces the partials in a fixed order (strided per
   // thread, then a fixed tree), so the sums are the same in every run
   double m = 0, f = 0;
   const volatile double* pf = MODE == 1 ? a.part_fl1 : a.part_fl2;
-  for (int q = t; q < nb; q += SP_THREADS) {
+  for (int q = t; q < nparts; q += SP_THREADS) {
     if (MODE == 2) m = fmax(m, ((volatile double*)a.part_max)[q]);
     f += pf[q];
   }
@@ -354,11 +408,11 @@ __global__ void __launch_bounds__(SP_THREADS) k_split_cells(StageArgs a, SplitBu
     f += __shfl_down_sync(0xffffffffu, f, o);
   }
   __syncthreads();
-  if ((t & 31) == 0) { s_red[0][t >> 5] = m; s_red[1][t >> 5] = f; }
+  if ((t & 31) == 0) { sm.red[0][t >> 5] = m; sm.red[1][t >> 5] = f; }
   __syncthreads();
   if (t == 0) {
-    m = s_red[0][0]; f = s_red[1][0];
-    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, s_red[0][w]); f += s_red[1][w]; }
+    m = sm.red[0][0]; f = sm.red[1][0];
+    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, sm.red[0][w]); f += sm.red[1][w]; }
     if (MODE == 1) {
       ctl->floored1 = f;
     } else {
@@ -369,6 +423,18 @@ __global__ void __launch_bounds__(SP_THREADS) k_split_cells(StageArgs a, SplitBu
     }
     ctl->counter = 0;
   }
+}
+
+#ifndef SWE_SPLIT_CELLS_MIN_BLOCKS
+#define SWE_SPLIT_CELLS_MIN_BLOCKS 4
+#endif
+template <int MODE>
+__global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_CELLS_MIN_BLOCKS)
+k_split_cells(StageArgs a, SplitBufs s, Control* ctl) {
+  if (ctl->stop) return;
+  __shared__ CellsSmem sm;
+  split_cells_tile<MODE>(a, s, ctl, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
+                         gridDim.x * gridDim.y, sm);
 }
 
 }  // namespace
