@@ -20,6 +20,7 @@
 // limiter, Coriolis, scalar or per-cell Manning n.  No sponge or Flather.
 #include "../../include/swe_b200.h"
 #include "swe_kernels.cuh"
+#include "swe_split.cuh"
 #include "swe_adjoint_math.cuh"
 
 #include <cuda_runtime.h>
@@ -417,23 +418,6 @@ __global__ void k_adj_bc(int nx, int ny, double* lb, double* lh, double* lhu, do
   }
 }
 
-// Stage outputs recomputed for their masks.
-__global__ void k_stage1_pre(int N, const double* h, const double* hu, const double* hv, const double* rh,
-                             const double* rhu, const double* rhv, double dt, double* oh, double* ohu, double* ohv) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
-    oh[k] = h[k] + dt * rh[k]; ohu[k] = hu[k] + dt * rhu[k]; ohv[k] = hv[k] + dt * rhv[k];
-  }
-}
-__global__ void k_stage2_pre(int N, const double* h0, const double* hu0, const double* hv0, const double* h,
-                             const double* hu, const double* hv, const double* rh, const double* rhu,
-                             const double* rhv, double dt, double* oh, double* ohu, double* ohv) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
-    oh[k] = 0.5 * (h0[k] + h[k] + dt * rh[k]);
-    ohu[k] = 0.5 * (hu0[k] + hu[k] + dt * rhu[k]);
-    ohv[k] = 0.5 * (hv0[k] + hv[k] + dt * rhv[k]);
-  }
-}
-
 // dryClean (src/swe.mjs:734-745) backwards, from the pre-clean depth:
 // a floored depth and zeroed momenta pass no adjoint.  Ghost outputs are
 // dead (the next ghost fill overwrites them), so their adjoints are cleared.
@@ -544,18 +528,6 @@ __global__ void k_init_state(int N, const double* b, const double* eta0, double*
   }
 }
 // dryClean's result (src/swe.mjs:734-745) on the interior, copying ghosts as they are.
-__global__ void k_clean_interior(int W, int H, double minDepth, const double* h, const double* hu, const double* hv,
-                                 double* oh, double* ohu, double* ohv) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < W * H; k += gridDim.x * blockDim.x) {
-    const int i = k % W, j = k / W;
-    double nh = h[k], nhu = hu[k], nhv = hv[k];
-    if (i >= 2 && i < W - 2 && j >= 2 && j < H - 2) {
-      if (nh < 0) nh = 0;
-      if (nh <= minDepth) { nhu = 0; nhv = 0; }
-    }
-    oh[k] = nh; ohu[k] = nhu; ohv[k] = nhv;
-  }
-}
 // The stage combinations backwards, three fields at once.
 // A = 0.5 (W1 + B + dt R2):  lB = 0.5 lA, lR = 0.5 dt lA, lA <- 0.5 lA (= lW1).
 __global__ void k_split_stage2(int N, double dt, double* lA0, double* lA1, double* lA2, double* lB0, double* lB1,
@@ -587,8 +559,7 @@ struct swe_adjoint {
   cudaStream_t st = nullptr;
   std::vector<double*> allocs;
   double *b, *eta0, *nfield = nullptr, *geom;
-  double *A[3], *Bf[3], *X[3], *Ap[3], *Adc[3];           // state, stage buffers
-  double *R[4];                                           // residual scratch
+  double *A[3], *Bf[3], *X[3];                            // state, stage-1 output, segment state
   double *ckpt, *tape;                                    // checkpoints, one segment's tapes
   double *dts, *obs = nullptr, *J, *eta_series = nullptr;
   int* gk;
@@ -601,6 +572,9 @@ struct swe_adjoint {
   Control* ctl;
   int nblocks;
   dim3 grid;
+  swe::SplitBufs sb;               // the tiled stage kernels' fields
+  dim3 sgrid;
+  int pcap = 0;                    // partial slots per kind (the most tiles either kernel uses)
   bool forward_done = false;
   bool fixed_dt = false;         // forward uses the given dt sequence instead of maxDt()
   std::vector<double> dts_host;  // the dt sequence, read once per backward pass
@@ -634,7 +608,7 @@ StageArgs stage_args(const swe_adjoint* s, double* const* in, double* const* out
   a.minDepth = s->o.min_depth; a.eps4 = s->eps4; a.coriolis = s->o.coriolis;
   a.sph = 0; a.order = s->o.order; a.lim = s->o.limiter;
   a.manning = s->o.manning; a.nfield = s->nfield;
-  a.part_max = s->part; a.part_fl1 = s->part + s->nblocks; a.part_fl2 = s->part + 2 * s->nblocks;
+  a.part_max = s->part; a.part_fl1 = s->part + s->pcap; a.part_fl2 = s->part + 2 * s->pcap;
   a.nblocks = s->nblocks;
   return a;
 }
@@ -664,9 +638,13 @@ int fwd_step(swe_adjoint* s, double* const* X, bool auto_dt, int step_index) {
     k_set_dt<<<1, 32, 0, s->st>>>(s->ctl, s->dts, step_index);
   }
   swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, X), s->ctl, 0);
-  swe::k_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(stage_args(s, X, s->Bf), s->ctl);
+  const StageArgs a1 = stage_args(s, X, s->Bf);
+  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
+  swe::k_split_cells<1><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
   swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, s->Bf), s->ctl, 0);
-  swe::k_stage<2><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(stage_args(s, s->Bf, X), s->ctl);
+  const StageArgs a2 = stage_args(s, s->Bf, X);
+  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
+  swe::k_split_cells<2><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
   CU(cudaGetLastError());
   if (auto_dt) k_record_dt<<<1, 32, 0, s->st>>>(s->ctl, s->dts, step_index);
   return SWE_OK;
@@ -721,33 +699,25 @@ Tape tape_at(const swe_adjoint* s, int t) {
   return T;
 }
 
-// Step k forward from X (in place) and record its tape.
+// Step k forward from X (in place) and record its tape: the tiled stage
+// kernels write the limiter, the depth before dryClean and friction's input
+// as they go.
 int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
-  const int N = s->N, gb = G1(s);
-  const double dt = s->dts_host[k];
+  const int N = s->N;
   k_set_dt<<<1, 32, 0, s->st>>>(s->ctl, s->dts, k);
-  double* Bpre[3] = {T.hB, s->Adc[1], s->Adc[2]};
-  double* Apre[3] = {T.hA, s->Ap[1], s->Ap[2]};
   copy3(s, T.W1, X);
   swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, T.W1), s->ctl, 0);
-  StageArgs r1 = stage_args(s, T.W1, nullptr);
-  r1.rh = s->R[0]; r1.rhu = s->R[1]; r1.rhv = s->R[2]; r1.theta = T.th1;
-  swe::k_stage<0><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(r1, s->ctl);
-  k_stage1_pre<<<gb, 256, 0, s->st>>>(N, T.W1[0], T.W1[1], T.W1[2], s->R[0], s->R[1], s->R[2], dt,
-                                      Bpre[0], Bpre[1], Bpre[2]);
-  k_clean_interior<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, Bpre[0], Bpre[1], Bpre[2],
-                                          T.Bp[0], T.Bp[1], T.Bp[2]);
+  StageArgs a1 = stage_args(s, T.W1, T.Bp);
+  a1.tape_th = T.th1; a1.tape_hpre = T.hB;
+  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
+  swe::k_split_cells<1><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
   swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, T.Bp), s->ctl, 0);
-  StageArgs r2 = stage_args(s, T.Bp, nullptr);
-  r2.rh = s->R[0]; r2.rhu = s->R[1]; r2.rhv = s->R[2]; r2.theta = T.th2;
-  swe::k_stage<0><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(r2, s->ctl);
-  k_stage2_pre<<<gb, 256, 0, s->st>>>(N, T.W1[0], T.W1[1], T.W1[2], T.Bp[0], T.Bp[1], T.Bp[2],
-                                      s->R[0], s->R[1], s->R[2], dt, Apre[0], Apre[1], Apre[2]);
-  k_clean_interior<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, Apre[0], Apre[1], Apre[2],
-                                          T.Bf[0], T.Bf[1], T.Bf[2]);
-  copy3(s, X, T.Bf);
-  StageArgs fr = stage_args(s, X, X);
-  swe::k_friction<<<std::max(1, std::min(4096, (s->o.nx * s->o.ny + 255) / 256)), 256, 0, s->st>>>(fr, dt);
+  copy3(s, X, T.W1);                               // U0 of the in-place stage 2
+  StageArgs a2 = stage_args(s, T.Bp, X);
+  a2.tape_th = T.th2; a2.tape_hpre = T.hA;
+  for (int q = 0; q < 3; q++) a2.tape_pre[q] = T.Bf[q];
+  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
+  swe::k_split_cells<2><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
   cudaMemcpyAsync(T.hX, X[0], sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
   CU(cudaGetLastError());
   return SWE_OK;
@@ -826,10 +796,9 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
   s->b = A(N); s->eta0 = A(N); s->geom = A((SWE_GEOM_NROWS + 3) * (size_t)s->H);
   if (manning_field) s->nfield = A(N);
   for (int q = 0; q < 3; q++) {
-    s->A[q] = A(N); s->Bf[q] = A(N); s->X[q] = A(N); s->Ap[q] = A(N); s->Adc[q] = A(N);
+    s->A[q] = A(N); s->Bf[q] = A(N); s->X[q] = A(N);
     s->lA[q] = A(N); s->lB[q] = A(N);
   }
-  for (int q = 0; q < 4; q++) s->R[q] = A(N);
   s->ckpt = A(3 * N * (size_t)s->nseg);
   s->tape = nullptr;               // allocated by the first backward pass
   s->dts = A(steps);
@@ -847,7 +816,13 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
   const int gx = (s->W + swe::SX - 1) / swe::SX, gy = (s->H + 31) / 32;
   s->grid = dim3(gx, gy);
   s->nblocks = gx * gy;
-  s->part = A(3 * (size_t)std::max(s->nblocks, 1024));
+  s->sgrid = dim3((s->W + swe::SPX - 1) / swe::SPX, (s->H + swe::SPY - 1) / swe::SPY);
+  s->pcap = std::max(std::max(s->nblocks, (int)(s->sgrid.x * s->sgrid.y)), 1024);
+  s->part = A(3 * (size_t)s->pcap);
+  {
+    double* spl = A((size_t)swe::SPLIT_FIELDS * N);
+    if (spl) s->sb = swe::split_bufs_at(spl, N);
+  }
   if (!ok || cudaMalloc(&s->ctl, sizeof(Control)) != cudaSuccess || cudaMalloc(&s->gk, sizeof(int) * n_gauges) != cudaSuccess)
     return bail(fail(SWE_ECUDA, "swe_adjoint_create: device allocation failed"));
   cudaMemsetAsync(s->ctl, 0, sizeof(Control), s->st);
