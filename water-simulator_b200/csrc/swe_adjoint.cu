@@ -8,13 +8,13 @@
 // `checkpoint_every` steps.  Backward: for each segment, newest first, the
 // segment is stepped forward again from its checkpoint (same kernels and
 // arithmetic, so every branch is the branch the forward pass took), and
-// each step's tape is kept: both stage inputs with their ghosts, both
+// each step's tape is kept as the tiled stage kernels write it: both stage
+// inputs with their ghosts, their velocities, slopes and face fluxes, both
 // positivity-limiter fields, the depths before each dryClean and friction's
-// input.  Then each step is reversed from its tape: the residual's
-// intermediates (velocities, slopes, face fluxes) are recomputed, and the
-// hand-written reverse kernels run friction, dryClean, the stage
-// combination, the residual and the ghost-cell maps backwards.  The initial
-// depth h = max(0, eta0 - b) is part of the map from b to J.
+// input.  Then each step is reversed from its tape: the hand-written reverse
+// kernels run friction, dryClean, the stage combination, the residual and
+// the ghost-cell maps backwards.  The initial depth h = max(0, eta0 - b) is
+// part of the map from b to J.
 //
 // Scope: Cartesian grids, walls (reflect) on every side, any order and
 // limiter, Coriolis, scalar or per-cell Manning n.  No sponge or Flather.
@@ -52,43 +52,16 @@ int fail(int code, const std::string& m) { swe_host::set_error(m); return code; 
 struct Inter {
   double *U, *V;
   double *s[8];          // sE0 sB0 sU0 sV0 (x), sE1 sB1 sU1 sV1 (y)
-  double *fx[5], *fy[5]; // M N T pL pR of the x face (k|k+1) and the y face (k|k+W)
+  double *fx[swe::SPLIT_FACE_FIELDS], *fy[swe::SPLIT_FACE_FIELDS];   // M, T, N + pL, N + pR of the
+                         // x face (k|k+1) and the y face (k|k+W), as the tiled face kernel writes them
 };
+using swe::F_M;
+using swe::F_T;
+using swe::F_NPL;
+using swe::F_NPR;
 
 struct Geo { int W, H, nx, ny; double minDepth, eps4, coriolis; int order, lim;
              const double *dxRow, *dyRowN, *dyRowS, *bedPhi; };
-
-__global__ void k_vel(Geo g, const double* h, const double* hu, const double* hv, double* U, double* V) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
-    const double hk = h[k];
-    if (hk == 0) { U[k] = swe::vel_num(hu[k], hk); V[k] = swe::vel_num(hv[k], hk); continue; }
-    const double den = swe::vel_den(hk, g.eps4);
-    U[k] = swe::vel_num(hu[k], hk) / den;
-    V[k] = swe::vel_num(hv[k], hk) / den;
-  }
-}
-
-// src/swe.mjs:364-411
-__global__ void k_slopes(Geo g, const double* b, const double* h, Inter it) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
-    const int i = k % g.W, j = k / g.W;
-    for (int d = 0; d < 2; d++) {
-      double sE = 0, sB = 0, sU = 0, sV = 0;
-      if (g.order >= 2 && i >= 1 && i < g.W - 1 && j >= 1 && j < g.H - 1) {
-        const int kp = d == 0 ? k + 1 : k + g.W, km = d == 0 ? k - 1 : k - g.W;
-        const double hk = h[k], bk = b[k], eC = bk + hk;
-        if (!(hk <= g.minDepth || h[kp] <= g.minDepth || h[km] <= g.minDepth)) {
-          const double eP = b[kp] + h[kp], eM = b[km] + h[km];
-          sE = swe::limiter(g.lim, eC - eM, eP - eC);
-          sB = swe::limiter(g.lim, bk - b[km], b[kp] - bk);
-          sU = swe::limiter(g.lim, it.U[k] - it.U[km], it.U[kp] - it.U[k]);
-          sV = swe::limiter(g.lim, it.V[k] - it.V[km], it.V[kp] - it.V[k]);
-        }
-      }
-      it.s[4 * d][k] = sE; it.s[4 * d + 1][k] = sB; it.s[4 * d + 2][k] = sU; it.s[4 * d + 3][k] = sV;
-    }
-  }
-}
 
 __device__ __forceinline__ bool xface_on(const Geo& g, int i, int j) { return j >= 2 && j < g.H - 2 && i >= 1 && i < g.W - 2; }
 __device__ __forceinline__ bool yface_on(const Geo& g, int i, int j) { return j >= 1 && j < g.H - 2 && i >= 2 && i < g.W - 2; }
@@ -102,26 +75,6 @@ __device__ __forceinline__ FaceIn yface_in(const Geo& g, const double* b, const 
   const int r = k + g.W;        // v normal, u transverse
   return {b[k], h[k], it.V[k], it.U[k], it.s[4][k], it.s[5][k], it.s[7][k], it.s[6][k],
           b[r], h[r], it.V[r], it.U[r], it.s[4][r], it.s[5][r], it.s[7][r], it.s[6][r]};
-}
-
-// src/swe.mjs:414-475
-__global__ void k_faces(Geo g, const double* b, const double* h, Inter it) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
-    const int i = k % g.W, j = k / g.W;
-    swe::Face fx = {0, 0, 0, 0, 0}, fy = {0, 0, 0, 0, 0};
-    if (xface_on(g, i, j)) {
-      const FaceIn x = xface_in(g, b, h, it, k);
-      fx = swe::face_flux(x.bL, x.hL, x.nL, x.tL, x.sEL, x.sBL, x.sNL, x.sTL,
-                          x.bR, x.hR, x.nR, x.tR, x.sER, x.sBR, x.sNR, x.sTR, g.minDepth);
-    }
-    if (yface_on(g, i, j)) {
-      const FaceIn y = yface_in(g, b, h, it, k);
-      fy = swe::face_flux(y.bL, y.hL, y.nL, y.tL, y.sEL, y.sBL, y.sNL, y.sTL,
-                          y.bR, y.hR, y.nR, y.tR, y.sER, y.sBR, y.sNR, y.sTR, g.minDepth);
-    }
-    it.fx[0][k] = fx.M; it.fx[1][k] = fx.N; it.fx[2][k] = fx.T; it.fx[3][k] = fx.pL; it.fx[4][k] = fx.pR;
-    it.fy[0][k] = fy.M; it.fy[1][k] = fy.N; it.fy[2][k] = fy.T; it.fy[3][k] = fy.pL; it.fy[4][k] = fy.pR;
-  }
 }
 
 // ---- adjoint of the residual -------------------------------------------------
@@ -142,7 +95,7 @@ __global__ void k_adj_faces_accum(Geo g, Inter it, const double* theta, AdjBuf a
     double lM = 0, lN = 0, lT = 0, lpL = 0, lpR = 0, lth = 0;
     if (xface_on(g, i, j)) {
       const int kL = k, kR = k + 1;
-      const double M = it.fx[0][k], N = it.fx[1][k], T = it.fx[2][k], pL = it.fx[3][k], pR = it.fx[4][k];
+      const double M = it.fx[F_M][k], T = it.fx[F_T][k], NpL = it.fx[F_NPL][k], NpR = it.fx[F_NPR][k];
       const double th = M >= 0 ? theta[kL] : theta[kR];
       const double inv = th / g.dxRow[j];
       lM = inv * (a.lR[0][kR] - a.lR[0][kL]);
@@ -150,7 +103,7 @@ __global__ void k_adj_faces_accum(Geo g, Inter it, const double* theta, AdjBuf a
       lT = inv * (a.lR[2][kR] - a.lR[2][kL]);
       lpL = -inv * a.lR[1][kL];
       lpR = inv * a.lR[1][kR];
-      const double linv = M * (a.lR[0][kR] - a.lR[0][kL]) + (N + pR) * a.lR[1][kR] - (N + pL) * a.lR[1][kL] +
+      const double linv = M * (a.lR[0][kR] - a.lR[0][kL]) + NpR * a.lR[1][kR] - NpL * a.lR[1][kL] +
                           T * (a.lR[2][kR] - a.lR[2][kL]);
       lth = linv / g.dxRow[j];
     }
@@ -158,7 +111,7 @@ __global__ void k_adj_faces_accum(Geo g, Inter it, const double* theta, AdjBuf a
     lM = 0; lN = 0; lT = 0; lpL = 0; lpR = 0; lth = 0;
     if (yface_on(g, i, j)) {
       const int kL = k, kR = k + g.W;
-      const double M = it.fy[0][k], N = it.fy[1][k], T = it.fy[2][k], pL = it.fy[3][k], pR = it.fy[4][k];
+      const double M = it.fy[F_M][k], T = it.fy[F_T][k], NpL = it.fy[F_NPL][k], NpR = it.fy[F_NPR][k];
       const double th = M >= 0 ? theta[kL] : theta[kR];
       const double invL = th / g.dyRowN[j], invR = th / g.dyRowS[j + 1];
       // rh[kL] -= M invL; rhv[kL] -= (N + pL) invL; rhu[kL] -= T invL; rh[kR] += M invR; ...
@@ -167,8 +120,8 @@ __global__ void k_adj_faces_accum(Geo g, Inter it, const double* theta, AdjBuf a
       lT = invR * a.lR[1][kR] - invL * a.lR[1][kL];
       lpL = -invL * a.lR[2][kL];
       lpR = invR * a.lR[2][kR];
-      const double linvL = -(M * a.lR[0][kL] + (N + pL) * a.lR[2][kL] + T * a.lR[1][kL]);
-      const double linvR = M * a.lR[0][kR] + (N + pR) * a.lR[2][kR] + T * a.lR[1][kR];
+      const double linvL = -(M * a.lR[0][kL] + NpL * a.lR[2][kL] + T * a.lR[1][kL]);
+      const double linvR = M * a.lR[0][kR] + NpR * a.lR[2][kR] + T * a.lR[1][kR];
       lth = linvL / g.dyRowN[j] + linvR / g.dyRowS[j + 1];
     }
     a.lFy[0][k] = lM; a.lFy[1][k] = lN; a.lFy[2][k] = lT; a.lFy[3][k] = lpL; a.lFy[4][k] = lpR; a.lthy[k] = lth;
@@ -566,7 +519,6 @@ struct swe_adjoint {
   int* gmeta = nullptr;          // gauge groups by cell: cells, offsets, gauge indices
   int ngroups = 0;
   double *lA[3], *lB[3], *lb, *ln;
-  Inter it;
   AdjBuf ab;
   double *part;
   Control* ctl;
@@ -657,18 +609,17 @@ void copy3(swe_adjoint* s, double* const* dst, double* const* src) {
 
 // R^T: given ab.lR (adjoint of rh, rhu, rhv over all cells) at state X (ghosts
 // filled), add into lX (h, hu, hv) and lb.
-int residual_adjoint(swe_adjoint* s, double* const* X, const double* theta, double dt, double* const* lX) {
+// `it` holds the velocities, slopes and faces of X, as the tape recorded them.
+int residual_adjoint(swe_adjoint* s, double* const* X, const Inter& it, const double* theta, double dt,
+                     double* const* lX) {
   const Geo g = geo_of(s);
   const int gb = G1(s);
-  k_vel<<<gb, 256, 0, s->st>>>(g, X[0], X[1], X[2], s->it.U, s->it.V);
-  k_slopes<<<gb, 256, 0, s->st>>>(g, s->b, X[0], s->it);
-  k_faces<<<gb, 256, 0, s->st>>>(g, s->b, X[0], s->it);
-  k_adj_faces_accum<<<gb, 256, 0, s->st>>>(g, s->it, theta, s->ab);
-  k_adj_theta<<<gb, 256, 0, s->st>>>(g, s->it, X[0], dt, s->ab);
+  k_adj_faces_accum<<<gb, 256, 0, s->st>>>(g, it, theta, s->ab);
+  k_adj_theta<<<gb, 256, 0, s->st>>>(g, it, X[0], dt, s->ab);
   k_adj_faces_core<<<std::min(148 * 4 * 4, (s->N + FACES_CORE_THREADS - 1) / FACES_CORE_THREADS),
-                     FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], s->it, s->ab);
-  k_adj_cells<<<gb, 256, 0, s->st>>>(g, s->b, X[0], X[1], X[2], s->it, s->ab, lX[1], lX[2]);
-  k_adj_cells_final<<<gb, 256, 0, s->st>>>(g, X[0], X[1], X[2], s->it, s->ab, s->lb, lX[0], lX[1], lX[2]);
+                     FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, s->ab);
+  k_adj_cells<<<gb, 256, 0, s->st>>>(g, s->b, X[0], X[1], X[2], it, s->ab, lX[1], lX[2]);
+  k_adj_cells_final<<<gb, 256, 0, s->st>>>(g, X[0], X[1], X[2], it, s->ab, s->lb, lX[0], lX[1], lX[2]);
   CU(cudaGetLastError());
   return SWE_OK;
 }
@@ -687,8 +638,21 @@ struct Tape {
   double* hA;      // stage-2 depth before dryClean
   double* Bf[3];   // friction's input
   double* hX;      // the step's output depth (the misfit reads it)
+  Inter it1, it2;  // velocities, slopes and faces of the two stage inputs
 };
-constexpr int TAPE_FIELDS = 14;
+constexpr int INTER_FIELDS = 2 + 8 + 2 * swe::SPLIT_FACE_FIELDS;
+constexpr int TAPE_FIELDS = 14 + 2 * INTER_FIELDS;
+
+Inter inter_at(double* p, size_t N) {
+  Inter it;
+  it.U = p; it.V = p + N;
+  for (int q = 0; q < 8; q++) it.s[q] = p + (2 + q) * N;
+  for (int q = 0; q < swe::SPLIT_FACE_FIELDS; q++) {
+    it.fx[q] = p + (10 + q) * N;
+    it.fy[q] = p + (10 + swe::SPLIT_FACE_FIELDS + q) * N;
+  }
+  return it;
+}
 
 Tape tape_at(const swe_adjoint* s, int t) {
   double* p = s->tape + (size_t)t * TAPE_FIELDS * s->N;
@@ -696,7 +660,20 @@ Tape tape_at(const swe_adjoint* s, int t) {
   Tape T;
   for (int q = 0; q < 3; q++) { T.W1[q] = p + q * N; T.Bp[q] = p + (5 + q) * N; T.Bf[q] = p + (10 + q) * N; }
   T.th1 = p + 3 * N; T.hB = p + 4 * N; T.th2 = p + 8 * N; T.hA = p + 9 * N; T.hX = p + 13 * N;
+  T.it1 = inter_at(p + 14 * N, N);
+  T.it2 = inter_at(p + (14 + INTER_FIELDS) * N, N);
   return T;
+}
+
+// The tiled kernels' buffers for a stage whose faces, slopes and velocities
+// go to the tape (the source terms stay in the handle's scratch).
+swe::SplitBufs tape_bufs(const swe_adjoint* s, const Inter& it) {
+  swe::SplitBufs b = s->sb;
+  for (int q = 0; q < swe::SPLIT_FACE_FIELDS; q++) { b.fx[q] = it.fx[q]; b.fy[q] = it.fy[q]; }
+  for (int q = 0; q < 8; q++) b.sl[q] = it.s[q];
+  b.U = it.U;
+  b.V = it.V;
+  return b;
 }
 
 // Step k forward from X (in place) and record its tape: the tiled stage
@@ -709,15 +686,17 @@ int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
   swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, T.W1), s->ctl, 0);
   StageArgs a1 = stage_args(s, T.W1, T.Bp);
   a1.tape_th = T.th1; a1.tape_hpre = T.hB;
-  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
-  swe::k_split_cells<1><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
+  const swe::SplitBufs b1 = tape_bufs(s, T.it1);
+  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, b1, s->ctl);
+  swe::k_split_cells<1><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, b1, s->ctl);
   swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, T.Bp), s->ctl, 0);
   copy3(s, X, T.W1);                               // U0 of the in-place stage 2
   StageArgs a2 = stage_args(s, T.Bp, X);
   a2.tape_th = T.th2; a2.tape_hpre = T.hA;
   for (int q = 0; q < 3; q++) a2.tape_pre[q] = T.Bf[q];
-  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
-  swe::k_split_cells<2><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
+  const swe::SplitBufs b2 = tape_bufs(s, T.it2);
+  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, b2, s->ctl);
+  swe::k_split_cells<2><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, b2, s->ctl);
   cudaMemcpyAsync(T.hX, X[0], sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
   CU(cudaGetLastError());
   return SWE_OK;
@@ -737,14 +716,14 @@ int reverse_step(swe_adjoint* s, int k, const Tape& T) {
   // A = 0.5 (W1 + Bp + dt R2): lB = 0.5 lA, lR2 = 0.5 dt lA, lW1 = 0.5 lA
   k_split_stage2<<<gb, 256, 0, s->st>>>(N, dt, lA[0], lA[1], lA[2], lB[0], lB[1], lB[2], s->ab.lR[0],
                                         s->ab.lR[1], s->ab.lR[2]);
-  int rc = residual_adjoint(s, T.Bp, T.th2, dt, lB);
+  int rc = residual_adjoint(s, T.Bp, T.it2, T.th2, dt, lB);
   if (rc) return rc;
   k_adj_bc<<<adjbc_blocks(s), 256, 0, s->st>>>(s->o.nx, s->o.ny, s->lb, lB[0], lB[1], lB[2]);
   k_adj_dryclean<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, T.hB, lB[0], lB[1], lB[2]);
   // B = W1 + dt R1 (all cells): lW1 += lB, lR1 = dt lB
   k_split_stage1<<<gb, 256, 0, s->st>>>(N, dt, lB[0], lB[1], lB[2], lA[0], lA[1], lA[2], s->ab.lR[0],
                                         s->ab.lR[1], s->ab.lR[2]);
-  rc = residual_adjoint(s, T.W1, T.th1, dt, lA);
+  rc = residual_adjoint(s, T.W1, T.it1, T.th1, dt, lA);
   if (rc) return rc;
   k_adj_bc<<<adjbc_blocks(s), 256, 0, s->st>>>(s->o.nx, s->o.ny, s->lb, lA[0], lA[1], lA[2]);
   CU(cudaGetLastError());
@@ -806,9 +785,7 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
   s->eta_series = A((size_t)steps * n_gauges);
   s->J = A(1);
   s->lb = A(N); s->ln = A(N);
-  s->it.U = A(N); s->it.V = A(N);
-  for (int q = 0; q < 8; q++) s->it.s[q] = A(N);
-  for (int q = 0; q < 5; q++) { s->it.fx[q] = A(N); s->it.fy[q] = A(N); s->ab.lFx[q] = A(N); s->ab.lFy[q] = A(N); }
+  for (int q = 0; q < 5; q++) { s->ab.lFx[q] = A(N); s->ab.lFy[q] = A(N); }
   for (int q = 0; q < 3; q++) s->ab.lR[q] = A(N);
   s->ab.lthx = A(N); s->ab.lthy = A(N); s->ab.lout = A(N); s->ab.lhth = A(N);
   for (int q = 0; q < 16; q++) { s->ab.gx[q] = A(N); s->ab.gy[q] = A(N); s->ab.gs[q] = A(N); }

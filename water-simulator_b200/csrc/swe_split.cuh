@@ -48,6 +48,10 @@ struct SplitBufs {
   double* fy[SPLIT_FACE_FIELDS];   // y face (k|k+W)
   double* tb[3];                   // bed term x, bed term y, geometric source
   double* U;                       // cell velocity u (spherical Coriolis)
+  // optional, for the adjoint's tape: every cell's slopes (x: eta, b, u, v;
+  // then y) and velocity v; with them set, u is written for every cell too
+  double* sl[8];
+  double* V;
 };
 
 // The SPLIT_FIELDS fields of one grid, `stride` doubles apart from `base`.
@@ -59,6 +63,8 @@ __host__ __forceinline__ SplitBufs split_bufs_at(double* base, size_t stride) {
   }
   for (int q = 0; q < 3; q++) b.tb[q] = base + (2 * SPLIT_FACE_FIELDS + q) * stride;
   b.U = base + (2 * SPLIT_FACE_FIELDS + 3) * stride;
+  for (int q = 0; q < 8; q++) b.sl[q] = nullptr;
+  b.V = nullptr;
   return b;
 }
 
@@ -96,7 +102,13 @@ __device__ __forceinline__ void split_faces_cell(const StageArgs& a, const Split
     }
   }
   s.tb[0][k] = tb0; s.tb[1][k] = tb1; s.tb[2][k] = tg;
-  if (sph) s.U[k] = Uk;
+  if (s.sl[0]) {
+    for (int q = 0; q < 4; q++) { s.sl[q][k] = sm.xs[q][ly][lx]; s.sl[4 + q][k] = sm.ys[q][ly][lx]; }
+    s.U[k] = Uk;
+    s.V[k] = Vk;
+  } else if (sph) {
+    s.U[k] = Uk;
+  }
 
   // east x face (k|k+1)
   Face fx = {0, 0, 0, 0, 0};
