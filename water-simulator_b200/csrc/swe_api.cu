@@ -274,9 +274,14 @@ int launch_bc(swe_sim* s, double* const* f, int respect_stop) {
 int ensure_split(swe_sim* s) {
   if (s->d_split) return SWE_OK;
   const size_t N = s->N;
-  CU(cudaMalloc(&s->d_split, sizeof(double) * swe::SPLIT_FIELDS * N));
-  CU(cudaMemsetAsync(s->d_split, 0, sizeof(double) * swe::SPLIT_FIELDS * N, s->st));
+  const size_t ntiles = (size_t)s->sgrid.x * s->sgrid.y;
+  const size_t doubles = swe::SPLIT_FIELDS * N + (ntiles + 1) / 2;       // + one int flag per tile
+  CU(cudaMalloc(&s->d_split, sizeof(double) * doubles));
+  CU(cudaMemsetAsync(s->d_split, 0, sizeof(double) * doubles, s->st));
   s->sb = swe::split_bufs_at(s->d_split, N);
+  s->sb.dry = reinterpret_cast<int*>(s->d_split + swe::SPLIT_FIELDS * N);
+  s->sb.ntx = (int)s->sgrid.x;
+  s->sb.nty = (int)s->sgrid.y;
   return SWE_OK;
 }
 

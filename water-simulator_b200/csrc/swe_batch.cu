@@ -132,6 +132,11 @@ namespace {
 
 size_t round_up(size_t n) { return (n + 31) & ~size_t(31); }   // 256-byte multiples
 
+// Tiles of a basin in the tiled pair's 32 x 8 tiling.
+size_t split_tiles(int W, int H) {
+  return (size_t)((W + swe::SPX - 1) / swe::SPX) * ((H + swe::SPY - 1) / swe::SPY);
+}
+
 // Partial slots a basin needs: one per tile at the finest tiling either
 // stage implementation uses (4-row fused tiles, or 32 x 8 tiles).
 size_t part_slots(int W, int H) {
@@ -317,7 +322,7 @@ int swe_batch_create(int n, const swe_options* opts, const double* const* b, con
     // b, A (3), B (3), the tiled pair's fields, metric rows, partial slots
     // (3 x one per tile, for the most tiles either kernel uses)
     total += round_up(N) * (7 + swe::SPLIT_FIELDS) + round_up((size_t)(SWE_GEOM_NROWS + 3) * s->H[q]) +
-             round_up(3 * part_slots(s->W[q], s->H[q]));
+             round_up(3 * part_slots(s->W[q], s->H[q])) + round_up((split_tiles(s->W[q], s->H[q]) + 1) / 2);
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
@@ -380,6 +385,9 @@ int swe_batch_create(int n, const swe_options* opts, const double* const* b, con
     B.bcB = bc; B.bcB.h = Bf[0]; B.bcB.hu = Bf[1]; B.bcB.hv = Bf[2];
     B.ctl = s->ctls + q;
     B.sp = swe::split_bufs_at(spl, rN);
+    B.sp.dry = reinterpret_cast<int*>(parts + round_up(3 * pcap));   // one flag per 32 x 8 tile
+    B.sp.ntx = (s->W[q] + swe::SPX - 1) / swe::SPX;
+    B.sp.nty = (Hq + swe::SPY - 1) / swe::SPY;
     B.prep.mode = 1; B.prep.dt_host = 0; B.prep.cfl = o.cfl; B.prep.t_end = INFINITY;
   }
   int rc = build_tiles(s);

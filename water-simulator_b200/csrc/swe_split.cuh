@@ -25,6 +25,16 @@
 // every tile of its tile list.  Face arrays are indexed by their left /
 // lower cell and are zero where no face exists, so the limiter reads them
 // unconditionally.
+//
+// Dry tiles.  When every cell of a tile and its one-cell halo has h exactly
+// 0, every face the tile owns is exactly +0 (both sides dry, so HLLC and
+// both pressure corrections vanish), every slope is 0, and its source terms
+// are +-0.  The face kernel then writes only the tile's dry flag; the cell
+// kernel reads a face or source term of a flagged tile as +0 without
+// loading it, and skips the limiter of a tile whose 3 x 3 neighbourhood is
+// all flagged (theta is 1 when the faces are zero).  Sums of +-0 terms
+// round to the same doubles either way, so the results are unchanged bit
+// for bit; only the memory traffic of dry land goes.
 #pragma once
 
 #include "swe_kernels.cuh"
@@ -50,8 +60,11 @@ struct SplitBufs {
   double* U;                       // cell velocity u (spherical Coriolis)
   // optional, for the adjoint's tape: every cell's slopes (x: eta, b, u, v;
   // then y) and velocity v; with them set, u is written for every cell too
+  // (and no tile is skipped as dry)
   double* sl[8];
   double* V;
+  int* dry;                        // per tile: 1 when its faces were not written (dry), or null
+  int ntx, nty;                    // tiles per row and column of the grid
 };
 
 // The SPLIT_FIELDS fields of one grid, `stride` doubles apart from `base`.
@@ -65,6 +78,8 @@ __host__ __forceinline__ SplitBufs split_bufs_at(double* base, size_t stride) {
   b.U = base + (2 * SPLIT_FACE_FIELDS + 3) * stride;
   for (int q = 0; q < 8; q++) b.sl[q] = nullptr;
   b.V = nullptr;
+  b.dry = nullptr;
+  b.ntx = b.nty = 0;
   return b;
 }
 
@@ -141,6 +156,7 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
   const int t = threadIdx.x;
 
   // state and velocities of the tile and its halo (zero outside the grid)
+  int dryHere = 1;
   for (int q = t; q < SSX * SSY; q += SP_THREADS) {
     const int ly = q / SSX, lx = q - ly * SSX;
     const int gi = i0 - 1 + lx, gj = j0 - 1 + ly;
@@ -157,8 +173,11 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
       }
     }
     sm.b[ly][lx] = b; sm.h[ly][lx] = h; sm.U[ly][lx] = U; sm.V[ly][lx] = V;
+    if (!(h == 0)) dryHere = 0;
   }
-  __syncthreads();
+  const bool allDry = __syncthreads_and(dryHere) && s.dry && !s.sl[0];
+  if (s.dry && t == 0) s.dry[ty * s.ntx + tx] = allDry ? 1 : 0;
+  if (allDry) return;                           // uniform across the CTA
 
   // x slopes (src/swe.mjs:364-411, d = 0)
   for (int q = t; q < SPY * (SPX + 1); q += SP_THREADS) {
@@ -214,14 +233,33 @@ __global__ void __launch_bounds__(SP_THREADS, 3) k_split_faces(StageArgs a, Spli
   split_faces_tile(a, s, blockIdx.x, blockIdx.y, sm);
 }
 
+struct CellsSmem {
+  double th[SPY + 2][SPX + 2];
+  double red[2][SP_THREADS / 32];
+  int dry[3][3];                  // dry flags of the tile's 3 x 3 neighbourhood
+  bool last;
+};
+
+// A face / source-term value owned by cell (gi, gj) of the 3 x 3 tile
+// neighbourhood of the tile at (i0, j0): +0 when its tile was dry.
+__device__ __forceinline__ double split_load(const CellsSmem& sm, int i0, int j0, int gi, int gj,
+                                             const double* arr, int k) {
+  const int c = gi < i0 ? 0 : (gi >= i0 + SPX ? 2 : 1);
+  const int r = gj < j0 ? 0 : (gj >= j0 + SPY ? 2 : 1);
+  return sm.dry[r][c] ? 0.0 : arr[k];
+}
+
 // Positivity limiter of cell (gi, gj) from its four faces' mass fluxes
 // (src/swe.mjs:511-529), with the same conservative pre-test as stage_tile.
-__device__ __forceinline__ double split_theta(const StageArgs& a, const SplitBufs& s, double dt, int gi, int gj) {
+__device__ __forceinline__ double split_theta(const StageArgs& a, const SplitBufs& s, const CellsSmem& sm,
+                                              int i0, int j0, double dt, int gi, int gj) {
   const int W = a.W, H = a.H;
   if (!(dt > 0 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1)) return 1;
   const int k = gj * W + gi;
-  const double fxE = s.fx[F_M][k], fxW = s.fx[F_M][k - 1];
-  const double fyN = s.fy[F_M][k], fyS = s.fy[F_M][k - W];
+  const double fxE = split_load(sm, i0, j0, gi, gj, s.fx[F_M], k);
+  const double fxW = split_load(sm, i0, j0, gi - 1, gj, s.fx[F_M], k - 1);
+  const double fyN = split_load(sm, i0, j0, gi, gj, s.fy[F_M], k);
+  const double fyS = split_load(sm, i0, j0, gi, gj - 1, s.fy[F_M], k - W);
   const double avail = a.h[k];
   const double est = ((fxE > 0 ? fxE : 0) - (fxW < 0 ? fxW : 0)) * a.m.rdxRow[gj]
                    + (fyN > 0 ? fyN : 0) * a.m.rdyRowN[gj] - (fyS < 0 ? fyS : 0) * a.m.rdyRowS[gj];
@@ -236,12 +274,6 @@ __device__ __forceinline__ double split_theta(const StageArgs& a, const SplitBuf
   }
   return th;
 }
-
-struct CellsSmem {
-  double th[SPY + 2][SPX + 2];
-  double red[2][SP_THREADS / 32];
-  bool last;
-};
 
 // Limiter, gather, update and epilogue of the tile (tx, ty), which holds
 // partial slot `part` of the `nparts` of its grid; the last tile of the
@@ -260,9 +292,18 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
   const bool bedOn = order2 || sph;
   const bool corOn = sph || (a.coriolis != 0 && a.coriolis == a.coriolis);
 
+  if (t < 9) {
+    const int r = t / 3, c = t - 3 * r, txn = tx - 1 + c, tyn = ty - 1 + r;
+    int f = 1;                                    // outside the grid: no faces there
+    if (txn >= 0 && txn < s.ntx && tyn >= 0 && tyn < s.nty) f = s.dry ? s.dry[tyn * s.ntx + txn] : 0;
+    sm.dry[r][c] = f;
+  }
+  __syncthreads();
+  const bool allDry = sm.dry[0][0] & sm.dry[0][1] & sm.dry[0][2] & sm.dry[1][0] & sm.dry[1][1] &
+                      sm.dry[1][2] & sm.dry[2][0] & sm.dry[2][1] & sm.dry[2][2];
   for (int q = t; q < (SPX + 2) * (SPY + 2); q += SP_THREADS) {
     const int ly = q / (SPX + 2), lx = q - ly * (SPX + 2);
-    sm.th[ly][lx] = split_theta(a, s, dt, i0 - 1 + lx, j0 - 1 + ly);
+    sm.th[ly][lx] = allDry ? 1.0 : split_theta(a, s, sm, i0, j0, dt, i0 - 1 + lx, j0 - 1 + ly);
   }
   __syncthreads();
 
@@ -277,14 +318,18 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
     const bool hasS = colY && gj - 1 >= 1 && gj - 1 < H - 2, hasN = colY && gj >= 1 && gj < H - 2;
     const bool interior = colY && rowX;
     double wM = 0, wT = 0, wN = 0, eM = 0, eT = 0, eN = 0, sM = 0, sT = 0, sN = 0, nM = 0, nT = 0, nN = 0;
-    if (hasW) { wM = s.fx[F_M][k - 1]; wT = s.fx[F_T][k - 1]; wN = s.fx[F_NPR][k - 1]; }
-    if (hasE) { eM = s.fx[F_M][k]; eT = s.fx[F_T][k]; eN = s.fx[F_NPL][k]; }
-    if (hasS) { sM = s.fy[F_M][k - W]; sT = s.fy[F_T][k - W]; sN = s.fy[F_NPR][k - W]; }
-    if (hasN) { nM = s.fy[F_M][k]; nT = s.fy[F_T][k]; nN = s.fy[F_NPL][k]; }
+    const bool dW = sm.dry[1][lx == 0 ? 0 : 1], dS = sm.dry[ly == 0 ? 0 : 1][1], dC = sm.dry[1][1];
+    if (hasW && !dW) { wM = s.fx[F_M][k - 1]; wT = s.fx[F_T][k - 1]; wN = s.fx[F_NPR][k - 1]; }
+    if (hasE && !dC) { eM = s.fx[F_M][k]; eT = s.fx[F_T][k]; eN = s.fx[F_NPL][k]; }
+    if (hasS && !dS) { sM = s.fy[F_M][k - W]; sT = s.fy[F_T][k - W]; sN = s.fy[F_NPR][k - W]; }
+    if (hasN && !dC) { nM = s.fy[F_M][k]; nT = s.fy[F_T][k]; nN = s.fy[F_NPL][k]; }
     const double hin = a.h[k], huin = a.hu[k], hvin = a.hv[k];
     double tb0 = 0, tb1 = 0, tg = 0, Uk = 0;
-    if (interior && bedOn) { tb0 = s.tb[0][k]; tb1 = s.tb[1][k]; if (sph) tg = s.tb[2][k]; }
-    if (interior && sph) Uk = s.U[k];
+    if (interior && bedOn && !dC) { tb0 = s.tb[0][k]; tb1 = s.tb[1][k]; if (sph) tg = s.tb[2][k]; }
+    if (interior && sph) {
+      if (!dC) Uk = s.U[k];
+      else Uk = vel_num(huin, hin);               // h is 0 here: the face kernel's u
+    }
     double U0h = 0, U0hu = 0, U0hv = 0;
     if (MODE == 2) { U0h = a.oh[k]; U0hu = a.ohu[k]; U0hv = a.ohv[k]; }
     const double thC = sm.th[ly + 1][lx + 1];
