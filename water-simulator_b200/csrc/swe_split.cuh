@@ -294,8 +294,11 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
 
   if (t < 9) {
     const int r = t / 3, c = t - 3 * r, txn = tx - 1 + c, tyn = ty - 1 + r;
-    int f = 1;                                    // outside the grid: no faces there
-    if (txn >= 0 && txn < s.ntx && tyn >= 0 && tyn < s.nty) f = s.dry ? s.dry[tyn * s.ntx + txn] : 0;
+    int f = 0;                                    // no flags: nothing is skipped
+    if (s.dry) {
+      f = 1;                                      // outside the grid: no faces there
+      if (txn >= 0 && txn < s.ntx && tyn >= 0 && tyn < s.nty) f = s.dry[tyn * s.ntx + txn];
+    }
     sm.dry[r][c] = f;
   }
   __syncthreads();
