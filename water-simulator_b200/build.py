@@ -4,6 +4,7 @@ The library is compiled with -fmad=false: no multiply-add is contracted, so
 the device arithmetic rounds operation by operation like the reference's
 JavaScript engine (the parity build of the step).
 """
+import glob
 import os
 import subprocess
 import sys
@@ -12,8 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libswe_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("swe_api.cu", "swe_batch.cu", "swe_adjoint.cu",
                                                     "swe_noalloc.cu", "swe_gridlands.cu", "swe_render.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("swe_kernels.cuh", "swe_math.cuh",
-                                                          "swe_adjoint_math.cuh")] + [
+DEPS = SOURCES + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [
     os.path.join(HERE, "..", "include", "swe_b200.h")]
 
 NVCC_FLAGS = [
