@@ -593,10 +593,12 @@ int fwd_step(swe_adjoint* s, double* const* X, bool auto_dt, int step_index) {
   const StageArgs a1 = stage_args(s, X, s->Bf);
   swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
   swe::k_split_cells<1><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
+  swe::k_split_close<1><<<1, swe::SP_THREADS, 0, s->st>>>(a1, s->ctl, (int)(s->sgrid.x * s->sgrid.y));
   swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, s->Bf), s->ctl, 0);
   const StageArgs a2 = stage_args(s, s->Bf, X);
   swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
   swe::k_split_cells<2><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
+  swe::k_split_close<2><<<1, swe::SP_THREADS, 0, s->st>>>(a2, s->ctl, (int)(s->sgrid.x * s->sgrid.y));
   CU(cudaGetLastError());
   if (auto_dt) k_record_dt<<<1, 32, 0, s->st>>>(s->ctl, s->dts, step_index);
   return SWE_OK;
@@ -689,6 +691,7 @@ int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
   const swe::SplitBufs b1 = tape_bufs(s, T.it1);
   swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, b1, s->ctl);
   swe::k_split_cells<1><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, b1, s->ctl);
+  swe::k_split_close<1><<<1, swe::SP_THREADS, 0, s->st>>>(a1, s->ctl, (int)(s->sgrid.x * s->sgrid.y));
   swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, T.Bp), s->ctl, 0);
   copy3(s, X, T.W1);                               // U0 of the in-place stage 2
   StageArgs a2 = stage_args(s, T.Bp, X);
@@ -697,6 +700,7 @@ int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
   const swe::SplitBufs b2 = tape_bufs(s, T.it2);
   swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, b2, s->ctl);
   swe::k_split_cells<2><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, b2, s->ctl);
+  swe::k_split_close<2><<<1, swe::SP_THREADS, 0, s->st>>>(a2, s->ctl, (int)(s->sgrid.x * s->sgrid.y));
   cudaMemcpyAsync(T.hX, X[0], sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
   CU(cudaGetLastError());
   return SWE_OK;

@@ -291,6 +291,7 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a) {
   if (s->stage_impl == 1) {
     swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, s->sb, s->d_ctl);
     swe::k_split_cells<MODE><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, s->sb, s->d_ctl);
+    swe::k_split_close<MODE><<<1, swe::SP_THREADS, 0, s->st>>>(a, s->d_ctl, (int)(s->sgrid.x * s->sgrid.y));
   } else {
     swe::k_stage<MODE><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a, s->d_ctl);
   }

@@ -91,7 +91,7 @@ k_batch_split_cells(BatchBasin* basins, const BatchTile* tiles, int ntiles) {
     const BatchTile tile = tiles[t];
     const BatchBasin& B = basins[tile.basin];
     const StageArgs& a = MODE == 1 ? B.s1 : B.s2;
-    if (!B.ctl->stop) swe::split_cells_tile<MODE>(a, B.sp, B.ctl, tile.strip, tile.y0, tile.part, a.nblocks, sm);
+    if (!B.ctl->stop) swe::split_cells_tile<MODE>(a, B.sp, B.ctl, tile.strip, tile.y0, tile.part, a.nblocks, sm, true);
     __syncthreads();          // the next tile reuses the shared limiter tile
   }
 }

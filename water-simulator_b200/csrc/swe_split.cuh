@@ -275,12 +275,48 @@ __device__ __forceinline__ double split_theta(const StageArgs& a, const SplitBuf
   return th;
 }
 
+// The close of a stage by one block: the partials of its `nparts` tiles
+// reduced in a fixed order (strided per thread, then a fixed tree), so the
+// sums are the same in every run.
+template <int MODE>
+__device__ __forceinline__ void split_close_block(const StageArgs& a, Control* ctl, int nparts, CellsSmem& sm) {
+  const int t = threadIdx.x;
+  const double dt = ctl->dt;
+  double m = 0, f = 0;
+  const volatile double* pf = MODE == 1 ? a.part_fl1 : a.part_fl2;
+  for (int q = t; q < nparts; q += SP_THREADS) {
+    if (MODE == 2) m = fmax(m, ((volatile double*)a.part_max)[q]);
+    f += pf[q];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    f += __shfl_down_sync(0xffffffffu, f, o);
+  }
+  __syncthreads();
+  if ((t & 31) == 0) { sm.red[0][t >> 5] = m; sm.red[1][t >> 5] = f; }
+  __syncthreads();
+  if (t == 0) {
+    m = sm.red[0][0]; f = sm.red[1][0];
+    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, sm.red[0][w]); f += sm.red[1][w]; }
+    if (MODE == 1) {
+      ctl->floored1 = f;
+    } else {
+      ctl->next_max = m;
+      ctl->mass_floored = ctl->floored1 + f;
+      ctl->t = ctl->t + dt;
+      ctl->steps = ctl->steps + 1;
+    }
+    ctl->counter = 0;
+  }
+}
+
 // Limiter, gather, update and epilogue of the tile (tx, ty), which holds
-// partial slot `part` of the `nparts` of its grid; the last tile of the
-// grid to finish closes the step.  Every thread of the CTA calls it.
+// partial slot `part` of the `nparts` of its grid.  With `ticket`, the last
+// tile of the grid to finish closes the step; without, the step is closed
+// by k_split_close after the launch.  Every thread of the CTA calls it.
 template <int MODE>
 __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const SplitBufs& s, Control* ctl, int tx,
-                                                 int ty, int part, int nparts, CellsSmem& sm) {
+                                                 int ty, int part, int nparts, CellsSmem& sm, bool ticket) {
   static_assert(MODE == 1 || MODE == 2, "stages only");
   const int W = a.W, H = a.H;
   const int i0 = tx * SPX, j0 = ty * SPY;
@@ -448,41 +484,17 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
     for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, sm.red[0][w]); f += sm.red[1][w]; }
     if (MODE == 1) a.part_fl1[part] = f;
     else { a.part_max[part] = m; a.part_fl2[part] = f; }
-    __threadfence();
-    const unsigned int ticket = atomicAdd(&ctl->counter, 1u);
-    sm.last = (ticket == (unsigned int)(nparts - 1));
+    if (ticket) {
+      __threadfence();
+      const unsigned int tk = atomicAdd(&ctl->counter, 1u);
+      sm.last = (tk == (unsigned int)(nparts - 1));
+    }
   }
+  if (!ticket) return;
   __syncthreads();
   if (!sm.last) return;                         // uniform across the CTA
   __threadfence();
-  // the whole last block reduces the partials in a fixed order (strided per
-  // thread, then a fixed tree), so the sums are the same in every run
-  double m = 0, f = 0;
-  const volatile double* pf = MODE == 1 ? a.part_fl1 : a.part_fl2;
-  for (int q = t; q < nparts; q += SP_THREADS) {
-    if (MODE == 2) m = fmax(m, ((volatile double*)a.part_max)[q]);
-    f += pf[q];
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-    f += __shfl_down_sync(0xffffffffu, f, o);
-  }
-  __syncthreads();
-  if ((t & 31) == 0) { sm.red[0][t >> 5] = m; sm.red[1][t >> 5] = f; }
-  __syncthreads();
-  if (t == 0) {
-    m = sm.red[0][0]; f = sm.red[1][0];
-    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, sm.red[0][w]); f += sm.red[1][w]; }
-    if (MODE == 1) {
-      ctl->floored1 = f;
-    } else {
-      ctl->next_max = m;
-      ctl->mass_floored = ctl->floored1 + f;
-      ctl->t = ctl->t + dt;
-      ctl->steps = ctl->steps + 1;
-    }
-    ctl->counter = 0;
-  }
+  split_close_block<MODE>(a, ctl, nparts, sm);
 }
 
 #ifndef SWE_SPLIT_CELLS_MIN_BLOCKS
@@ -494,7 +506,16 @@ k_split_cells(StageArgs a, SplitBufs s, Control* ctl) {
   if (ctl->stop) return;
   __shared__ CellsSmem sm;
   split_cells_tile<MODE>(a, s, ctl, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
-                         gridDim.x * gridDim.y, sm);
+                         gridDim.x * gridDim.y, sm, false);
+}
+
+// Closes the stage k_split_cells left open: one block, no atomics (a
+// ticket shared by every tile of a large grid serialises in L2).
+template <int MODE>
+__global__ void __launch_bounds__(SP_THREADS) k_split_close(StageArgs a, Control* ctl, int nparts) {
+  if (ctl->stop) return;
+  __shared__ CellsSmem sm;
+  split_close_block<MODE>(a, ctl, nparts, sm);
 }
 
 }  // namespace
