@@ -613,6 +613,8 @@ def run_adjoint(args):
         sim.close()
     adj = swe.MisfitAdjoint(n, n, 10.0, c["b"], c["eta0"], **kw)
     adj.set_observations(obs)
+    adj.forward()                     # warm-up gradient: the tape is allocated on the first backward
+    adj.backward()
     (J, _), t_fwd = timed(adj.stream(), adj.forward)
     (gb, gn), t_bwd = timed(adj.stream(), adj.backward)
     dts = adj.dt_sequence()

@@ -160,30 +160,47 @@ __global__ void k_adj_theta(Geo g, Inter it, const double* h, double dt, AdjBuf 
 // face_flux's reverse.
 // 128 registers at most: 16 warps per SM instead of the 8 that 140 leave.
 constexpr int FACES_CORE_THREADS = 128;
-__global__ void __launch_bounds__(FACES_CORE_THREADS, 4)
+#ifndef SWE_FACES_CORE_MIN_BLOCKS
+#define SWE_FACES_CORE_MIN_BLOCKS 4
+#endif
+// One launch for the x faces and one for the y faces: one face per thread
+// fits 128 registers without spilling (16 warps per SM) and measured
+// faster than both faces per thread at 128 or 168 registers.
+#ifndef SWE_FACES_CORE_SPLIT
+#define SWE_FACES_CORE_SPLIT 1
+#endif
+// WHICH: 0 the x face of each cell, 1 its y face, 2 both.
+template <int WHICH>
+__global__ void __launch_bounds__(FACES_CORE_THREADS, SWE_FACES_CORE_MIN_BLOCKS)
 k_adj_faces_core(Geo g, const double* b, const double* h, Inter it, AdjBuf a) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
     const int i = k % g.W, j = k / g.W;
-    FaceIn gx = {}, gy = {};
-    if (xface_on(g, i, j)) {
-      double lM = a.lFx[0][k];
-      const double M = it.fx[0][k];
-      if (M > 0) lM += a.lout[k] / g.dxRow[j];
-      if (M < 0) lM -= a.lout[k + 1] / g.dxRow[j];
-      gx = swe::adj::face_rev(xface_in(g, b, h, it, k), g.minDepth, lM, a.lFx[1][k], a.lFx[2][k],
-                              a.lFx[3][k], a.lFx[4][k]);
+    if (WHICH != 1) {
+      FaceIn gx = {};
+      if (xface_on(g, i, j)) {
+        double lM = a.lFx[0][k];
+        const double M = it.fx[0][k];
+        if (M > 0) lM += a.lout[k] / g.dxRow[j];
+        if (M < 0) lM -= a.lout[k + 1] / g.dxRow[j];
+        gx = swe::adj::face_rev(xface_in(g, b, h, it, k), g.minDepth, lM, a.lFx[1][k], a.lFx[2][k],
+                                a.lFx[3][k], a.lFx[4][k]);
+      }
+      const double* px = &gx.bL;
+      for (int q = 0; q < 16; q++) a.gx[q][k] = px[q];
     }
-    if (yface_on(g, i, j)) {
-      double lM = a.lFy[0][k];
-      const double M = it.fy[0][k];
-      if (M > 0) lM += a.lout[k] / g.dyRowN[j];
-      if (M < 0) lM -= a.lout[k + g.W] / g.dyRowS[j + 1];
-      gy = swe::adj::face_rev(yface_in(g, b, h, it, k), g.minDepth, lM, a.lFy[1][k], a.lFy[2][k],
-                              a.lFy[3][k], a.lFy[4][k]);
+    if (WHICH != 0) {
+      FaceIn gy = {};
+      if (yface_on(g, i, j)) {
+        double lM = a.lFy[0][k];
+        const double M = it.fy[0][k];
+        if (M > 0) lM += a.lout[k] / g.dyRowN[j];
+        if (M < 0) lM -= a.lout[k + g.W] / g.dyRowS[j + 1];
+        gy = swe::adj::face_rev(yface_in(g, b, h, it, k), g.minDepth, lM, a.lFy[1][k], a.lFy[2][k],
+                                a.lFy[3][k], a.lFy[4][k]);
+      }
+      const double* py = &gy.bL;
+      for (int q = 0; q < 16; q++) a.gy[q][k] = py[q];
     }
-    const double* px = &gx.bL;
-    const double* py = &gy.bL;
-    for (int q = 0; q < 16; q++) { a.gx[q][k] = px[q]; a.gy[q][k] = py[q]; }
   }
 }
 
@@ -618,8 +635,13 @@ int residual_adjoint(swe_adjoint* s, double* const* X, const Inter& it, const do
   const int gb = G1(s);
   k_adj_faces_accum<<<gb, 256, 0, s->st>>>(g, it, theta, s->ab);
   k_adj_theta<<<gb, 256, 0, s->st>>>(g, it, X[0], dt, s->ab);
-  k_adj_faces_core<<<std::min(148 * 4 * 4, (s->N + FACES_CORE_THREADS - 1) / FACES_CORE_THREADS),
-                     FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, s->ab);
+  const int fcb = std::min(148 * 4 * 4, (s->N + FACES_CORE_THREADS - 1) / FACES_CORE_THREADS);
+  if (SWE_FACES_CORE_SPLIT) {
+    k_adj_faces_core<0><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, s->ab);
+    k_adj_faces_core<1><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, s->ab);
+  } else {
+    k_adj_faces_core<2><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, s->ab);
+  }
   k_adj_cells<<<gb, 256, 0, s->st>>>(g, s->b, X[0], X[1], X[2], it, s->ab, lX[1], lX[2]);
   k_adj_cells_final<<<gb, 256, 0, s->st>>>(g, X[0], X[1], X[2], it, s->ab, s->lb, lX[0], lX[1], lX[2]);
   CU(cudaGetLastError());
