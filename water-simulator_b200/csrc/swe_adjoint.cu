@@ -80,80 +80,85 @@ __device__ __forceinline__ FaceIn yface_in(const Geo& g, const double* b, const 
 // ---- adjoint of the residual -------------------------------------------------
 struct AdjBuf {
   double *lR[3];          // adjoints of rh, rhu, rhv (input)
-  double *lFx[5], *lFy[5];// face-output adjoints (M N T pL pR)
-  double *lthx, *lthy;    // theta adjoint a face sends to its upwind cell
-  double *lout, *lhth;    // positivity limiter: adjoint of `out`, and the depth term
   double *gx[16], *gy[16];// face-input adjoints (FaceIn order)
   double *gs[16];         // per cell: (dslope/da, dslope/dc) x adjoint, 8 slopes
   double *dir[4];         // per cell: direct adjoints of b, h, U, V
 };
 
-// Face accumulation (src/swe.mjs:530-555) backwards.
-__global__ void k_adj_faces_accum(Geo g, Inter it, const double* theta, AdjBuf a) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
-    const int i = k % g.W, j = k / g.W;
-    double lM = 0, lN = 0, lT = 0, lpL = 0, lpR = 0, lth = 0;
-    if (xface_on(g, i, j)) {
-      const int kL = k, kR = k + 1;
-      const double M = it.fx[F_M][k], T = it.fx[F_T][k], NpL = it.fx[F_NPL][k], NpR = it.fx[F_NPR][k];
-      const double th = M >= 0 ? theta[kL] : theta[kR];
-      const double inv = th / g.dxRow[j];
-      lM = inv * (a.lR[0][kR] - a.lR[0][kL]);
-      lN = inv * (a.lR[1][kR] - a.lR[1][kL]);
-      lT = inv * (a.lR[2][kR] - a.lR[2][kL]);
-      lpL = -inv * a.lR[1][kL];
-      lpR = inv * a.lR[1][kR];
-      const double linv = M * (a.lR[0][kR] - a.lR[0][kL]) + NpR * a.lR[1][kR] - NpL * a.lR[1][kL] +
-                          T * (a.lR[2][kR] - a.lR[2][kL]);
-      lth = linv / g.dxRow[j];
-    }
-    a.lFx[0][k] = lM; a.lFx[1][k] = lN; a.lFx[2][k] = lT; a.lFx[3][k] = lpL; a.lFx[4][k] = lpR; a.lthx[k] = lth;
-    lM = 0; lN = 0; lT = 0; lpL = 0; lpR = 0; lth = 0;
-    if (yface_on(g, i, j)) {
-      const int kL = k, kR = k + g.W;
-      const double M = it.fy[F_M][k], T = it.fy[F_T][k], NpL = it.fy[F_NPL][k], NpR = it.fy[F_NPR][k];
-      const double th = M >= 0 ? theta[kL] : theta[kR];
-      const double invL = th / g.dyRowN[j], invR = th / g.dyRowS[j + 1];
-      // rh[kL] -= M invL; rhv[kL] -= (N + pL) invL; rhu[kL] -= T invL; rh[kR] += M invR; ...
-      lM = invR * a.lR[0][kR] - invL * a.lR[0][kL];
-      lN = invR * a.lR[2][kR] - invL * a.lR[2][kL];
-      lT = invR * a.lR[1][kR] - invL * a.lR[1][kL];
-      lpL = -invL * a.lR[2][kL];
-      lpR = invR * a.lR[2][kR];
-      const double linvL = -(M * a.lR[0][kL] + NpL * a.lR[2][kL] + T * a.lR[1][kL]);
-      const double linvR = M * a.lR[0][kR] + NpR * a.lR[2][kR] + T * a.lR[1][kR];
-      lth = linvL / g.dyRowN[j] + linvR / g.dyRowS[j + 1];
-    }
-    a.lFy[0][k] = lM; a.lFy[1][k] = lN; a.lFy[2][k] = lT; a.lFy[3][k] = lpL; a.lFy[4][k] = lpR; a.lthy[k] = lth;
+// Face accumulation (src/swe.mjs:530-555) backwards, one face at a time:
+// the adjoints of the face's outputs (M, N, T, pL, pR) and the part of the
+// positivity limiter's adjoint it sends to its upwind cell.
+struct FaceAdj { double lM, lN, lT, lpL, lpR, lth; };
+
+__device__ __forceinline__ FaceAdj xface_adj(const Geo& g, const Inter& it, const double* theta, const AdjBuf& a,
+                                             int k, int i, int j) {
+  FaceAdj f = {0, 0, 0, 0, 0, 0};
+  if (!xface_on(g, i, j)) return f;
+  const int kL = k, kR = k + 1;
+  const double M = it.fx[F_M][k], T = it.fx[F_T][k], NpL = it.fx[F_NPL][k], NpR = it.fx[F_NPR][k];
+  const double th = M >= 0 ? theta[kL] : theta[kR];
+  const double inv = th / g.dxRow[j];
+  f.lM = inv * (a.lR[0][kR] - a.lR[0][kL]);
+  f.lN = inv * (a.lR[1][kR] - a.lR[1][kL]);
+  f.lT = inv * (a.lR[2][kR] - a.lR[2][kL]);
+  f.lpL = -inv * a.lR[1][kL];
+  f.lpR = inv * a.lR[1][kR];
+  const double linv = M * (a.lR[0][kR] - a.lR[0][kL]) + NpR * a.lR[1][kR] - NpL * a.lR[1][kL] +
+                      T * (a.lR[2][kR] - a.lR[2][kL]);
+  f.lth = linv / g.dxRow[j];
+  return f;
+}
+
+__device__ __forceinline__ FaceAdj yface_adj(const Geo& g, const Inter& it, const double* theta, const AdjBuf& a,
+                                             int k, int i, int j) {
+  FaceAdj f = {0, 0, 0, 0, 0, 0};
+  if (!yface_on(g, i, j)) return f;
+  const int kL = k, kR = k + g.W;
+  const double M = it.fy[F_M][k], T = it.fy[F_T][k], NpL = it.fy[F_NPL][k], NpR = it.fy[F_NPR][k];
+  const double th = M >= 0 ? theta[kL] : theta[kR];
+  const double invL = th / g.dyRowN[j], invR = th / g.dyRowS[j + 1];
+  // rh[kL] -= M invL; rhv[kL] -= (N + pL) invL; rhu[kL] -= T invL; rh[kR] += M invR; ...
+  f.lM = invR * a.lR[0][kR] - invL * a.lR[0][kL];
+  f.lN = invR * a.lR[2][kR] - invL * a.lR[2][kL];
+  f.lT = invR * a.lR[1][kR] - invL * a.lR[1][kL];
+  f.lpL = -invL * a.lR[2][kL];
+  f.lpR = invR * a.lR[2][kR];
+  const double linvL = -(M * a.lR[0][kL] + NpL * a.lR[2][kL] + T * a.lR[1][kL]);
+  const double linvR = M * a.lR[0][kR] + NpR * a.lR[2][kR] + T * a.lR[1][kR];
+  f.lth = linvL / g.dyRowN[j] + linvR / g.dyRowS[j + 1];
+  return f;
+}
+
+// Positivity limiter (src/swe.mjs:511-529) backwards for cell k: the
+// adjoint of its outgoing flux budget and of its depth.  Both are zero
+// unless the limiter fired (theta < 1), so callers only come here then.
+__device__ __forceinline__ void theta_adj(const Geo& g, const Inter& it, const double* theta, const double* h,
+                                          double dt, const AdjBuf& a, int k, double& lout, double& lh) {
+  lout = 0; lh = 0;
+  const int i = k % g.W, j = k / g.W;
+  if (!(dt > 0 && i >= 1 && i < g.W - 1 && j >= 1 && j < g.H - 1)) return;
+  double lth = 0;
+  if (it.fx[F_M][k] >= 0) lth += xface_adj(g, it, theta, a, k, i, j).lth;              // east face, upwind = k
+  if (it.fx[F_M][k - 1] < 0) lth += xface_adj(g, it, theta, a, k - 1, i - 1, j).lth;   // west face
+  if (it.fy[F_M][k] >= 0) lth += yface_adj(g, it, theta, a, k, i, j).lth;              // north face
+  if (it.fy[F_M][k - g.W] < 0) lth += yface_adj(g, it, theta, a, k - g.W, i, j - 1).lth;   // south face
+  double out = 0;
+  if (it.fx[F_M][k] > 0) out += it.fx[F_M][k] / g.dxRow[j];
+  if (it.fx[F_M][k - 1] < 0) out -= it.fx[F_M][k - 1] / g.dxRow[j];
+  if (it.fy[F_M][k] > 0) out += it.fy[F_M][k] / g.dyRowN[j];
+  if (it.fy[F_M][k - g.W] < 0) out -= it.fy[F_M][k - g.W] / g.dyRowS[j];
+  const double avail = h[k];
+  if (out * dt > avail && avail > 0) {                 // theta = avail / (out dt)
+    lh = lth / (out * dt);
+    lout = -lth * avail / (out * out * dt);
   }
 }
 
-// Positivity limiter (src/swe.mjs:511-529) backwards: theta's adjoint is
-// gathered from the faces this cell is upwind of.
-__global__ void k_adj_theta(Geo g, Inter it, const double* h, double dt, AdjBuf a) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
-    const int i = k % g.W, j = k / g.W;
-    double lout = 0, lh = 0;
-    if (dt > 0 && i >= 1 && i < g.W - 1 && j >= 1 && j < g.H - 1) {
-      double lth = 0;
-      if (it.fx[0][k] >= 0) lth += a.lthx[k];              // east face, upwind = k
-      if (it.fx[0][k - 1] < 0) lth += a.lthx[k - 1];       // west face
-      if (it.fy[0][k] >= 0) lth += a.lthy[k];              // north face
-      if (it.fy[0][k - g.W] < 0) lth += a.lthy[k - g.W];   // south face
-      double out = 0;
-      if (it.fx[0][k] > 0) out += it.fx[0][k] / g.dxRow[j];
-      if (it.fx[0][k - 1] < 0) out -= it.fx[0][k - 1] / g.dxRow[j];
-      if (it.fy[0][k] > 0) out += it.fy[0][k] / g.dyRowN[j];
-      if (it.fy[0][k - g.W] < 0) out -= it.fy[0][k - g.W] / g.dyRowS[j];
-      const double avail = h[k];
-      if (out * dt > avail && avail > 0) {                 // theta = avail / (out dt)
-        lh = lth / (out * dt);
-        lout = -lth * avail / (out * out * dt);
-      }
-    }
-    a.lout[k] = lout;
-    a.lhth[k] = lh;
-  }
+__device__ __forceinline__ double lout_of(const Geo& g, const Inter& it, const double* theta, const double* h,
+                                          double dt, const AdjBuf& a, int k) {
+  double lo = 0, lh = 0;
+  if (theta[k] < 1) theta_adj(g, it, theta, h, dt, a, k, lo, lh);
+  return lo;
 }
 
 // The faces backwards: limiter terms into the flux adjoint, then
@@ -172,18 +177,18 @@ constexpr int FACES_CORE_THREADS = 128;
 // WHICH: 0 the x face of each cell, 1 its y face, 2 both.
 template <int WHICH>
 __global__ void __launch_bounds__(FACES_CORE_THREADS, SWE_FACES_CORE_MIN_BLOCKS)
-k_adj_faces_core(Geo g, const double* b, const double* h, Inter it, AdjBuf a) {
+k_adj_faces_core(Geo g, const double* b, const double* h, Inter it, const double* theta, double dt, AdjBuf a) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
     const int i = k % g.W, j = k / g.W;
     if (WHICH != 1) {
       FaceIn gx = {};
       if (xface_on(g, i, j)) {
-        double lM = a.lFx[0][k];
-        const double M = it.fx[0][k];
-        if (M > 0) lM += a.lout[k] / g.dxRow[j];
-        if (M < 0) lM -= a.lout[k + 1] / g.dxRow[j];
-        gx = swe::adj::face_rev(xface_in(g, b, h, it, k), g.minDepth, lM, a.lFx[1][k], a.lFx[2][k],
-                                a.lFx[3][k], a.lFx[4][k]);
+        const FaceAdj f = xface_adj(g, it, theta, a, k, i, j);
+        double lM = f.lM;
+        const double M = it.fx[F_M][k];
+        if (M > 0) lM += lout_of(g, it, theta, h, dt, a, k) / g.dxRow[j];
+        if (M < 0) lM -= lout_of(g, it, theta, h, dt, a, k + 1) / g.dxRow[j];
+        gx = swe::adj::face_rev(xface_in(g, b, h, it, k), g.minDepth, lM, f.lN, f.lT, f.lpL, f.lpR);
       }
       const double* px = &gx.bL;
       for (int q = 0; q < 16; q++) a.gx[q][k] = px[q];
@@ -191,12 +196,12 @@ k_adj_faces_core(Geo g, const double* b, const double* h, Inter it, AdjBuf a) {
     if (WHICH != 0) {
       FaceIn gy = {};
       if (yface_on(g, i, j)) {
-        double lM = a.lFy[0][k];
-        const double M = it.fy[0][k];
-        if (M > 0) lM += a.lout[k] / g.dyRowN[j];
-        if (M < 0) lM -= a.lout[k + g.W] / g.dyRowS[j + 1];
-        gy = swe::adj::face_rev(yface_in(g, b, h, it, k), g.minDepth, lM, a.lFy[1][k], a.lFy[2][k],
-                                a.lFy[3][k], a.lFy[4][k]);
+        const FaceAdj f = yface_adj(g, it, theta, a, k, i, j);
+        double lM = f.lM;
+        const double M = it.fy[F_M][k];
+        if (M > 0) lM += lout_of(g, it, theta, h, dt, a, k) / g.dyRowN[j];
+        if (M < 0) lM -= lout_of(g, it, theta, h, dt, a, k + g.W) / g.dyRowS[j + 1];
+        gy = swe::adj::face_rev(yface_in(g, b, h, it, k), g.minDepth, lM, f.lN, f.lT, f.lpL, f.lpR);
       }
       const double* py = &gy.bL;
       for (int q = 0; q < 16; q++) a.gy[q][k] = py[q];
@@ -209,7 +214,7 @@ enum { F_BL, F_HL, F_NL, F_TL, F_SEL, F_SBL, F_SNL, F_STL, F_BR, F_HR, F_NR, F_T
 // Per cell: gather the faces' adjoints, add the bed term and Coriolis
 // backwards, then the limiter derivatives of each slope.
 __global__ void k_adj_cells(Geo g, const double* b, const double* h, const double* hu, const double* hv,
-                            Inter it, AdjBuf a, double* lhu, double* lhv) {
+                            Inter it, const double* theta, double dt, AdjBuf a, double* lhu, double* lhv) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
     const int i = k % g.W, j = k / g.W;
     double db = 0, dh = 0, dU = 0, dV = 0;
@@ -232,7 +237,11 @@ __global__ void k_adj_cells(Geo g, const double* b, const double* h, const doubl
       db += a.gy[F_BR][f]; dh += a.gy[F_HR][f]; dV += a.gy[F_NR][f]; dU += a.gy[F_TR][f];
       ls[4] += a.gy[F_SER][f]; ls[5] += a.gy[F_SBR][f]; ls[7] += a.gy[F_SNR][f]; ls[6] += a.gy[F_STR][f];
     }
-    dh += a.lhth[k];
+    {
+      double lo = 0, lh = 0;
+      if (theta[k] < 1) theta_adj(g, it, theta, h, dt, a, k, lo, lh);
+      dh += lh;
+    }
     double dhu = 0, dhv = 0;
     const bool interior = i >= 2 && i < g.W - 2 && j >= 2 && j < g.H - 2;
     if (interior && g.order >= 2) {                  // bed term, src/swe.mjs:570-598 (Cartesian)
@@ -633,16 +642,14 @@ int residual_adjoint(swe_adjoint* s, double* const* X, const Inter& it, const do
                      double* const* lX) {
   const Geo g = geo_of(s);
   const int gb = G1(s);
-  k_adj_faces_accum<<<gb, 256, 0, s->st>>>(g, it, theta, s->ab);
-  k_adj_theta<<<gb, 256, 0, s->st>>>(g, it, X[0], dt, s->ab);
   const int fcb = std::min(148 * 4 * 4, (s->N + FACES_CORE_THREADS - 1) / FACES_CORE_THREADS);
   if (SWE_FACES_CORE_SPLIT) {
-    k_adj_faces_core<0><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, s->ab);
-    k_adj_faces_core<1><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, s->ab);
+    k_adj_faces_core<0><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, theta, dt, s->ab);
+    k_adj_faces_core<1><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, theta, dt, s->ab);
   } else {
-    k_adj_faces_core<2><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, s->ab);
+    k_adj_faces_core<2><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, theta, dt, s->ab);
   }
-  k_adj_cells<<<gb, 256, 0, s->st>>>(g, s->b, X[0], X[1], X[2], it, s->ab, lX[1], lX[2]);
+  k_adj_cells<<<gb, 256, 0, s->st>>>(g, s->b, X[0], X[1], X[2], it, theta, dt, s->ab, lX[1], lX[2]);
   k_adj_cells_final<<<gb, 256, 0, s->st>>>(g, X[0], X[1], X[2], it, s->ab, s->lb, lX[0], lX[1], lX[2]);
   CU(cudaGetLastError());
   return SWE_OK;
@@ -811,9 +818,7 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
   s->eta_series = A((size_t)steps * n_gauges);
   s->J = A(1);
   s->lb = A(N); s->ln = A(N);
-  for (int q = 0; q < 5; q++) { s->ab.lFx[q] = A(N); s->ab.lFy[q] = A(N); }
   for (int q = 0; q < 3; q++) s->ab.lR[q] = A(N);
-  s->ab.lthx = A(N); s->ab.lthy = A(N); s->ab.lout = A(N); s->ab.lhth = A(N);
   for (int q = 0; q < 16; q++) { s->ab.gx[q] = A(N); s->ab.gy[q] = A(N); s->ab.gs[q] = A(N); }
   for (int q = 0; q < 4; q++) s->ab.dir[q] = A(N);
   const int gx = (s->W + swe::SX - 1) / swe::SX, gy = (s->H + 31) / 32;
