@@ -91,20 +91,9 @@ k_batch_split_cells(BatchBasin* basins, const BatchTile* tiles, int ntiles) {
     const BatchTile tile = tiles[t];
     const BatchBasin& B = basins[tile.basin];
     const StageArgs& a = MODE == 1 ? B.s1 : B.s2;
-    if (!B.ctl->stop) swe::split_cells_tile<MODE>(a, B.sp, B.ctl, tile.strip, tile.y0, tile.part, a.nblocks, sm, false);
+    if (!B.ctl->stop) swe::split_cells_tile<MODE>(a, B.sp, B.ctl, tile.strip, tile.y0, tile.part, a.nblocks, sm, true);
     __syncthreads();          // the next tile reuses the shared limiter tile
   }
-}
-
-// One block per basin closes the stage from its tiles' partials (no
-// ticket shared by a basin's tiles).
-template <int MODE>
-__global__ void __launch_bounds__(swe::SP_THREADS) k_batch_split_close(BatchBasin* basins) {
-  const BatchBasin& B = basins[blockIdx.x];
-  if (B.ctl->stop) return;
-  __shared__ swe::CellsSmem sm;
-  const StageArgs& a = MODE == 1 ? B.s1 : B.s2;
-  swe::split_close_block<MODE>(a, B.ctl, a.nblocks, sm);
 }
 
 int fail(int code, const std::string& m) { swe_host::set_error(m); return code; }
@@ -222,7 +211,6 @@ int enqueue_batch_step(swe_batch* s) {
   if (s->impl == 1) {
     k_batch_split_faces<1><<<s->grid, swe::SP_THREADS, 0, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
     k_batch_split_cells<1><<<s->grid, swe::SP_THREADS, 0, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
-    k_batch_split_close<1><<<s->nb, swe::SP_THREADS, 0, s->st>>>(s->d_basins);
   } else {
     k_batch_stage<1><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
   }
@@ -232,7 +220,6 @@ int enqueue_batch_step(swe_batch* s) {
   if (s->impl == 1) {
     k_batch_split_faces<2><<<s->grid, swe::SP_THREADS, 0, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
     k_batch_split_cells<2><<<s->grid, swe::SP_THREADS, 0, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
-    k_batch_split_close<2><<<s->nb, swe::SP_THREADS, 0, s->st>>>(s->d_basins);
   } else {
     k_batch_stage<2><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(s->d_basins, s->d_tiles, s->ntiles);
   }
