@@ -73,7 +73,7 @@ k_batch_stage(BatchBasin* basins, const BatchTile* tiles, int ntiles) {
 // tile row) of that basin's 32 x 8 tiling; its partial slot closes the
 // basin's step exactly as in the single-grid kernels.
 template <int MODE>
-__global__ void __launch_bounds__(swe::SP_THREADS, 3)
+__global__ void __launch_bounds__(swe::SP_THREADS, SWE_SPLIT_FACES_MIN_BLOCKS)
 k_batch_split_faces(BatchBasin* basins, const BatchTile* tiles, int ntiles) {
   __shared__ swe::FacesSmem sm;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {

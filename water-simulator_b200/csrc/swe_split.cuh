@@ -227,7 +227,11 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(SP_THREADS, 3) k_split_faces(StageArgs a, SplitBufs s, Control* ctl) {
+#ifndef SWE_SPLIT_FACES_MIN_BLOCKS
+#define SWE_SPLIT_FACES_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_FACES_MIN_BLOCKS)
+k_split_faces(StageArgs a, SplitBufs s, Control* ctl) {
   if (ctl->stop) return;
   __shared__ FacesSmem sm;
   split_faces_tile(a, s, blockIdx.x, blockIdx.y, sm);
