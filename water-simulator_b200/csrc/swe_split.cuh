@@ -287,10 +287,29 @@ __device__ __forceinline__ void split_close_block(const StageArgs& a, Control* c
   const int t = threadIdx.x;
   const double dt = ctl->dt;
   double m = 0, f = 0;
-  const volatile double* pf = MODE == 1 ? a.part_fl1 : a.part_fl2;
-  for (int q = t; q < nparts; q += SP_THREADS) {
-    if (MODE == 2) m = fmax(m, ((volatile double*)a.part_max)[q]);
-    f += pf[q];
+  // The partials are read at L2 (__ldcg: another CTA of the same launch may
+  // have written them, and L1 is not coherent), CLOSE_BATCH loads in flight
+  // per thread; each thread still adds its slots q = t, t + 256, ... in
+  // increasing order.
+  constexpr int CLOSE_BATCH = 8;
+  const double* pf = MODE == 1 ? a.part_fl1 : a.part_fl2;
+  int q = t;
+  for (; q + (CLOSE_BATCH - 1) * SP_THREADS < nparts; q += CLOSE_BATCH * SP_THREADS) {
+    double vf[CLOSE_BATCH], vm[CLOSE_BATCH];
+#pragma unroll
+    for (int u = 0; u < CLOSE_BATCH; u++) {
+      vf[u] = __ldcg(pf + q + u * SP_THREADS);
+      if (MODE == 2) vm[u] = __ldcg(a.part_max + q + u * SP_THREADS);
+    }
+#pragma unroll
+    for (int u = 0; u < CLOSE_BATCH; u++) {
+      if (MODE == 2) m = fmax(m, vm[u]);
+      f += vf[u];
+    }
+  }
+  for (; q < nparts; q += SP_THREADS) {
+    if (MODE == 2) m = fmax(m, __ldcg(a.part_max + q));
+    f += __ldcg(pf + q);
   }
   for (int o = 16; o > 0; o >>= 1) {
     m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
