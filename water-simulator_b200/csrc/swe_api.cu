@@ -63,6 +63,7 @@ struct swe_sim {
   double dx, dy, eps4, R, dlam, dphi, totalArea;
   std::vector<double> geom[SWE_GEOM_NROWS];
   std::vector<double> recip[3];
+  int dryfold = 0;                                 // every reciprocal row finite
   cudaStream_t st = nullptr;
   double* d_b = nullptr;
   double* d_A[3] = {nullptr, nullptr, nullptr};
@@ -242,6 +243,7 @@ swe::StageArgs stage_args(const swe_sim* s, double* const* in, double* const* ou
   a.sponge_str = s->d_sponge; a.sponge_ref = s->sponge_ref;
   a.part_max = s->d_part; a.part_fl1 = s->d_part + s->part_cap; a.part_fl2 = s->d_part + 2 * s->part_cap;
   a.nblocks = s->nblocks;
+  a.dryfold = s->dryfold;
   return a;
 }
 
@@ -383,6 +385,8 @@ void fill_reciprocals(swe_sim* s) {
     s->recip[q].resize(s->H);
     for (int j = 0; j < s->H; j++) s->recip[q][j] = 1.0 / s->geom[src[q]][j];
   }
+  s->dryfold = 1;
+  for (int q = 0; q < 3; q++) s->dryfold &= swe::dry_fold_ok(s->recip[q].data(), s->recip[q].size());
 }
 
 int upload_geom(swe_sim* s) {

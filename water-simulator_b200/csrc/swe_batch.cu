@@ -363,6 +363,7 @@ int swe_batch_create(int n, const swe_options* opts, const double* const* b, con
     a.m.fRow = g + SWE_GEOM_FROW * Hq; a.m.tanPhi = g + SWE_GEOM_TANPHI * Hq;
     a.m.rdxRow = g + (SWE_GEOM_NROWS + 0) * Hq; a.m.rdyRowN = g + (SWE_GEOM_NROWS + 1) * Hq;
     a.m.rdyRowS = g + (SWE_GEOM_NROWS + 2) * Hq;
+    a.dryfold = swe::dry_fold_ok(geom[q].data() + (size_t)SWE_GEOM_NROWS * Hq, (size_t)3 * Hq);
     double Rv = 0;
     {
       std::vector<double> sc(6);

@@ -98,6 +98,9 @@ struct StageArgs {
   // the cell's positivity limiter, its depth before dryClean and (stage 2)
   // the state after dryClean that friction takes
   double* tape_th; double* tape_hpre; double* tape_pre[3];
+  // every reciprocal metric row (rdxRow, rdyRowN, rdyRowS) finite, so a
+  // face value of +0 times any of them is +0
+  int dryfold;
 };
 
 // ---------------------------------------------------------------------------

@@ -83,6 +83,23 @@ __host__ __forceinline__ SplitBufs split_bufs_at(double* base, size_t stride) {
   return b;
 }
 
+// Whether `n` reciprocal metric values are all finite (StageArgs::dryfold).
+__host__ inline int dry_fold_ok(const double* recip, size_t n) {
+  for (size_t q = 0; q < n; q++)
+    if (!(recip[q] - recip[q] == 0)) return 0;      // inf - inf and NaN - NaN are NaN
+  return 1;
+}
+
+// 8-byte global -> shared copy that runs asynchronously (cp.async, sm_80+):
+// a thread issues all of its copies, then waits once, so their latencies
+// overlap instead of adding up.  Only the issuing thread reads the copied
+// value, after cp_async_wait_all.
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 struct FacesSmem {
   double b[SSY][SSX], h[SSY][SSX], U[SSY][SSX], V[SSY][SSX];
   double xs[4][SPY][SPX + 1];                   // x slopes of cols i0 .. i0+SPX, rows j0 .. j0+SPY-1
@@ -155,29 +172,48 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
   const bool bedOn = order2 || sph;
   const int t = threadIdx.x;
 
-  // state and velocities of the tile and its halo (zero outside the grid)
+  // state of the tile and its halo (zero outside the grid): b, h, hu, hv
+  // copied into b, h, U, V with every copy of the thread in flight at once;
+  // once the tile is known to be wet, each thread turns the hu, hv it
+  // copied into velocities in place
   int dryHere = 1;
   for (int q = t; q < SSX * SSY; q += SP_THREADS) {
     const int ly = q / SSX, lx = q - ly * SSX;
     const int gi = i0 - 1 + lx, gj = j0 - 1 + ly;
-    double b = 0, h = 0, U = 0, V = 0;
     if (gi >= 0 && gi < W && gj >= 0 && gj < H) {
       const int k = gj * W + gi;
-      b = __ldg(a.b + k); h = __ldg(a.h + k);
-      const double hu = __ldg(a.hu + k), hv = __ldg(a.hv + k);
+      cp_async8(&sm.b[ly][lx], a.b + k);
+      cp_async8(&sm.h[ly][lx], a.h + k);
+      cp_async8(&sm.U[ly][lx], a.hu + k);
+      cp_async8(&sm.V[ly][lx], a.hv + k);
+    } else {
+      sm.b[ly][lx] = 0; sm.h[ly][lx] = 0; sm.U[ly][lx] = 0; sm.V[ly][lx] = 0;
+    }
+  }
+  cp_async_wait_all();
+  for (int q = t; q < SSX * SSY; q += SP_THREADS) {
+    const int ly = q / SSX, lx = q - ly * SSX;
+    if (!(sm.h[ly][lx] == 0)) dryHere = 0;     // zero outside the grid
+  }
+  const bool allDry = __syncthreads_and(dryHere) && s.dry && !s.sl[0];
+  if (s.dry && t == 0) s.dry[ty * s.ntx + tx] = allDry ? 1 : 0;
+  if (allDry) return;                           // uniform across the CTA
+  for (int q = t; q < SSX * SSY; q += SP_THREADS) {
+    const int ly = q / SSX, lx = q - ly * SSX;
+    const int gi = i0 - 1 + lx, gj = j0 - 1 + ly;
+    if (gi >= 0 && gi < W && gj >= 0 && gj < H) {
+      const double h = sm.h[ly][lx], hu = sm.U[ly][lx], hv = sm.V[ly][lx];
+      double U, V;
       if (h == 0) {                  // +-0 / den == +-0 and NaN / den == NaN: no division needed
         U = vel_num(hu, h); V = vel_num(hv, h);
       } else {
         const double den = vel_den(h, eps4);
         U = vel_num(hu, h) / den; V = vel_num(hv, h) / den;
       }
+      sm.U[ly][lx] = U; sm.V[ly][lx] = V;
     }
-    sm.b[ly][lx] = b; sm.h[ly][lx] = h; sm.U[ly][lx] = U; sm.V[ly][lx] = V;
-    if (!(h == 0)) dryHere = 0;
   }
-  const bool allDry = __syncthreads_and(dryHere) && s.dry && !s.sl[0];
-  if (s.dry && t == 0) s.dry[ty * s.ntx + tx] = allDry ? 1 : 0;
-  if (allDry) return;                           // uniform across the CTA
+  __syncthreads();
 
   // x slopes (src/swe.mjs:364-411, d = 0)
   for (int q = t; q < SPY * (SPX + 1); q += SP_THREADS) {
@@ -238,6 +274,7 @@ k_split_faces(StageArgs a, SplitBufs s, Control* ctl) {
 }
 
 struct CellsSmem {
+  double st[6][SP_THREADS];       // each thread's own cell: h, hu, hv, then U0 (stage 2)
   double th[SPY + 2][SPX + 2];
   double red[2][SP_THREADS / 32];
   int dry[3][3];                  // dry flags of the tile's 3 x 3 neighbourhood
@@ -333,6 +370,144 @@ __device__ __forceinline__ void split_close_block(const StageArgs& a, Control* c
   }
 }
 
+// One cell's gather, source terms, update and epilogue, adding to the
+// tile's partials.  DRY: the tile's 3 x 3 neighbourhood is flagged dry, so
+// every face the cell reads is +0 and theta is 1.  With finite reciprocal
+// metrics (StageArgs::dryfold) each face term is then +0 * (finite) = +-0
+// added to or taken from a +0 sum, and the bed terms are +0, so the sums
+// are +0 with or without them: DRY leaves them out and gives the same bits.
+template <int MODE, bool DRY>
+__device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& s, const CellsSmem& sm, int t,
+                                           int lx, int ly, int gi, int gj, double dt, double& locMax,
+                                           double& locFl) {
+  const int W = a.W, H = a.H;
+  const double dry = a.minDepth, eps4 = a.eps4;
+  const bool sph = a.sph != 0;
+  const bool bedOn = a.order >= 2 || sph;
+  const bool corOn = sph || (a.coriolis != 0 && a.coriolis == a.coriolis);
+  const int k = gj * W + gi;
+  // every load of the cell first, so they are in flight together
+  const bool rowX = gj >= 2 && gj < H - 2, colY = gi >= 2 && gi < W - 2;
+  const bool hasW = rowX && gi - 1 >= 1 && gi - 1 < W - 2, hasE = rowX && gi >= 1 && gi < W - 2;
+  const bool hasS = colY && gj - 1 >= 1 && gj - 1 < H - 2, hasN = colY && gj >= 1 && gj < H - 2;
+  const bool interior = colY && rowX;
+  double wM = 0, wT = 0, wN = 0, eM = 0, eT = 0, eN = 0, sM = 0, sT = 0, sN = 0, nM = 0, nT = 0, nN = 0;
+  const bool dW = sm.dry[1][lx == 0 ? 0 : 1], dS = sm.dry[ly == 0 ? 0 : 1][1], dC = sm.dry[1][1];
+  if (!DRY && hasW && !dW) { wM = s.fx[F_M][k - 1]; wT = s.fx[F_T][k - 1]; wN = s.fx[F_NPR][k - 1]; }
+  if (!DRY && hasE && !dC) { eM = s.fx[F_M][k]; eT = s.fx[F_T][k]; eN = s.fx[F_NPL][k]; }
+  if (!DRY && hasS && !dS) { sM = s.fy[F_M][k - W]; sT = s.fy[F_T][k - W]; sN = s.fy[F_NPR][k - W]; }
+  if (!DRY && hasN && !dC) { nM = s.fy[F_M][k]; nT = s.fy[F_T][k]; nN = s.fy[F_NPL][k]; }
+  cp_async_wait_all();
+  const double hin = sm.st[0][t], huin = sm.st[1][t], hvin = sm.st[2][t];
+  double tb0 = 0, tb1 = 0, tg = 0, Uk = 0;
+  if (!DRY && interior && bedOn && !dC) { tb0 = s.tb[0][k]; tb1 = s.tb[1][k]; if (sph) tg = s.tb[2][k]; }
+  if (interior && sph) {
+    if (!DRY && !dC) Uk = s.U[k];
+    else Uk = vel_num(huin, hin);               // h is 0 here: the face kernel's u
+  }
+  double U0h = 0, U0hu = 0, U0hv = 0;
+  if (MODE == 2) { U0h = sm.st[3][t]; U0hu = sm.st[4][t]; U0hv = sm.st[5][t]; }
+  const double thC = DRY ? 1.0 : sm.th[ly + 1][lx + 1];
+  const double rdx = a.m.rdxRow[gj], dxr = a.m.dxRow[gj];
+  double ah = 0, ahu = 0, ahv = 0;
+  if (!DRY && hasW) {                                       // west face, cell is its right side
+    const double thf = wM >= 0 ? sm.th[ly + 1][lx] : thC;
+    const double inv = thf == 1 ? rdx : thf / dxr;
+    ah += wM * inv; ahu += wN * inv; ahv += wT * inv;
+  }
+  if (!DRY && hasE) {                                       // east face, cell is its left side
+    const double thf = eM >= 0 ? thC : sm.th[ly + 1][lx + 2];
+    const double inv = thf == 1 ? rdx : thf / dxr;
+    ah -= eM * inv; ahu -= eN * inv; ahv -= eT * inv;
+  }
+  if (!DRY && hasS) {                                       // south face, cell is its upper side
+    const double thf = sM >= 0 ? sm.th[ly][lx + 1] : thC;
+    const double invR = thf == 1 ? a.m.rdyRowS[gj] : thf / a.m.dyRowS[gj];
+    ah += sM * invR; ahv += sN * invR; ahu += sT * invR;
+  }
+  if (!DRY && hasN) {                                       // north face, cell is its lower side
+    const double thf = nM >= 0 ? thC : sm.th[ly + 2][lx + 1];
+    const double invL = thf == 1 ? a.m.rdyRowN[gj] : thf / a.m.dyRowN[gj];
+    ah -= nM * invL; ahv -= nN * invL; ahu -= nT * invL;
+  }
+  if (interior) {
+    if (!DRY && bedOn) {
+      ahu += tb0;
+      ahv += tb1;
+      if (sph) ahv += tg;
+    }
+    if (sph) {
+      const double fe = a.m.fRow[gj] + Uk * (a.m.tanPhi[gj] / a.m.R);
+      ahu += fe * hvin;
+      ahv -= fe * huin;
+    } else if (corOn) {
+      ahu += a.coriolis * hvin;
+      ahv -= a.coriolis * huin;
+    }
+  }
+  if (a.tape_th) a.tape_th[k] = thC;
+  if (MODE == 1) {
+    double nh = hin + dt * ah, nhu = huin + dt * ahu, nhv = hvin + dt * ahv;
+    if (a.tape_hpre) a.tape_hpre[k] = nh;
+    if (interior) {                                 // dryClean, src/swe.mjs:734-745
+      if (nh < 0) { locFl -= nh; nh = 0; }
+      if (nh <= dry) { nhu = 0; nhv = 0; }
+    }
+    a.oh[k] = nh; a.ohu[k] = nhu; a.ohv[k] = nhv;
+  } else {
+    const double h0 = U0h, hu0 = U0hu, hv0 = U0hv;   // U0 (in place)
+    if (a.h0c) { a.h0c[k] = h0; a.hu0c[k] = hu0; a.hv0c[k] = hv0; }
+    double nh = 0.5 * (h0 + hin + dt * ah);
+    double nhu = 0.5 * (hu0 + huin + dt * ahu);
+    double nhv = 0.5 * (hv0 + hvin + dt * ahv);
+    if (a.tape_hpre) a.tape_hpre[k] = nh;
+    if (interior) {
+      if (nh < 0) { locFl -= nh; nh = 0; }
+      if (nh <= dry) { nhu = 0; nhv = 0; }
+      if (a.tape_pre[0]) { a.tape_pre[0][k] = nh; a.tape_pre[1][k] = nhu; a.tape_pre[2][k] = nhv; }
+      // friction, src/swe.mjs:659-704
+      const double n = a.nfield ? a.nfield[k] : a.manning;
+      const bool fricOn = a.nfield ? true : (n != 0 && n == n);
+      if (fricOn) {
+        if (nh <= dry) { nhu = 0; nhv = 0; }
+        else if (n != 0 && n == n) {
+          const double den = vel_den(nh, eps4);
+          const double u = vel_num(nhu, nh) / den, v = vel_num(nhv, nh) / den;
+          const double speed = hypot(u, v);
+          if (!(speed < 1e-14)) {
+            const double denom = 1 + dt * SWE_G * n * n * speed / pow(nh, 4.0 / 3.0);
+            nhu = nhu / denom;
+            nhv = nhv / denom;
+          }
+        }
+      }
+      // sponge, src/swe.mjs:1188-1197
+      if (a.sponge_width > 0) {
+        const int ii = gi - 2, jj = gj - 2;
+        int d;
+        if (a.sponge_side == 1) d = a.nx - 1 - ii; else if (a.sponge_side == 0) d = ii;
+        else if (a.sponge_side == 3) d = a.ny - 1 - jj; else d = jj;
+        if (d < a.sponge_width) {
+          const double f = jmin(1, a.sponge_str[d] * dt * 60);
+          const double target = jmax0(a.sponge_ref - __ldg(a.b + k));
+          nh = nh + (target - nh) * f;
+          nhu = nhu - nhu * f;
+          nhv = nhv - nhv * f;
+        }
+      }
+      // CFL rate of the final state, src/swe.mjs:632-647
+      if (!(nh <= dry)) {
+        const double cc = sqrt(SWE_G * nh);
+        const double den = vel_den(nh, eps4);
+        const double u = fabs(vel_num(nhu, nh) / den), v = fabs(vel_num(nhv, nh) / den);
+        const double sr5 = (u + cc) / dxr + (v + cc) / a.m.dyCFL[gj];
+        if (sr5 > locMax) locMax = sr5;
+      }
+    }
+    a.oh[k] = nh; a.ohu[k] = nhu; a.ohv[k] = nhv;
+  }
+}
+
 // Limiter, gather, update and epilogue of the tile (tx, ty), which holds
 // partial slot `part` of the `nparts` of its grid.  With `ticket`, the last
 // tile of the grid to finish closes the step; without, the step is closed
@@ -345,11 +520,22 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
   const int i0 = tx * SPX, j0 = ty * SPY;
   const int t = threadIdx.x;
   const double dt = ctl->dt;
-  const double dry = a.minDepth, eps4 = a.eps4;
-  const bool order2 = a.order >= 2;
-  const bool sph = a.sph != 0;
-  const bool bedOn = order2 || sph;
-  const bool corOn = sph || (a.coriolis != 0 && a.coriolis == a.coriolis);
+  const int lx = t % SPX, ly = t / SPX;
+  const int gi = i0 + lx, gj = j0 + ly;
+
+  // the cell's own state is copied first, in flight while the flags and
+  // the limiter are worked out
+  if (gi < W && gj < H) {
+    const int k = gj * W + gi;
+    cp_async8(&sm.st[0][t], a.h + k);
+    cp_async8(&sm.st[1][t], a.hu + k);
+    cp_async8(&sm.st[2][t], a.hv + k);
+    if (MODE == 2) {
+      cp_async8(&sm.st[3][t], a.oh + k);
+      cp_async8(&sm.st[4][t], a.ohu + k);
+      cp_async8(&sm.st[5][t], a.ohv + k);
+    }
+  }
 
   if (t < 9) {
     const int r = t / 3, c = t - 3 * r, txn = tx - 1 + c, tyn = ty - 1 + r;
@@ -363,148 +549,39 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
   __syncthreads();
   const bool allDry = sm.dry[0][0] & sm.dry[0][1] & sm.dry[0][2] & sm.dry[1][0] & sm.dry[1][1] &
                       sm.dry[1][2] & sm.dry[2][0] & sm.dry[2][1] & sm.dry[2][2];
-  for (int q = t; q < (SPX + 2) * (SPY + 2); q += SP_THREADS) {
-    const int ly = q / (SPX + 2), lx = q - ly * (SPX + 2);
-    sm.th[ly][lx] = allDry ? 1.0 : split_theta(a, s, sm, i0, j0, dt, i0 - 1 + lx, j0 - 1 + ly);
+  const bool fold = allDry && a.dryfold;          // uniform across the CTA
+  if (!fold) {
+    for (int q = t; q < (SPX + 2) * (SPY + 2); q += SP_THREADS) {
+      const int ly = q / (SPX + 2), lx = q - ly * (SPX + 2);
+      sm.th[ly][lx] = allDry ? 1.0 : split_theta(a, s, sm, i0, j0, dt, i0 - 1 + lx, j0 - 1 + ly);
+    }
+    __syncthreads();
   }
-  __syncthreads();
 
   double locMax = 0, locFl = 0;
-  const int lx = t % SPX, ly = t / SPX;
-  const int gi = i0 + lx, gj = j0 + ly;
   if (gi < W && gj < H) {
-    const int k = gj * W + gi;
-    // every load of the cell first, so they are in flight together
-    const bool rowX = gj >= 2 && gj < H - 2, colY = gi >= 2 && gi < W - 2;
-    const bool hasW = rowX && gi - 1 >= 1 && gi - 1 < W - 2, hasE = rowX && gi >= 1 && gi < W - 2;
-    const bool hasS = colY && gj - 1 >= 1 && gj - 1 < H - 2, hasN = colY && gj >= 1 && gj < H - 2;
-    const bool interior = colY && rowX;
-    double wM = 0, wT = 0, wN = 0, eM = 0, eT = 0, eN = 0, sM = 0, sT = 0, sN = 0, nM = 0, nT = 0, nN = 0;
-    const bool dW = sm.dry[1][lx == 0 ? 0 : 1], dS = sm.dry[ly == 0 ? 0 : 1][1], dC = sm.dry[1][1];
-    if (hasW && !dW) { wM = s.fx[F_M][k - 1]; wT = s.fx[F_T][k - 1]; wN = s.fx[F_NPR][k - 1]; }
-    if (hasE && !dC) { eM = s.fx[F_M][k]; eT = s.fx[F_T][k]; eN = s.fx[F_NPL][k]; }
-    if (hasS && !dS) { sM = s.fy[F_M][k - W]; sT = s.fy[F_T][k - W]; sN = s.fy[F_NPR][k - W]; }
-    if (hasN && !dC) { nM = s.fy[F_M][k]; nT = s.fy[F_T][k]; nN = s.fy[F_NPL][k]; }
-    const double hin = a.h[k], huin = a.hu[k], hvin = a.hv[k];
-    double tb0 = 0, tb1 = 0, tg = 0, Uk = 0;
-    if (interior && bedOn && !dC) { tb0 = s.tb[0][k]; tb1 = s.tb[1][k]; if (sph) tg = s.tb[2][k]; }
-    if (interior && sph) {
-      if (!dC) Uk = s.U[k];
-      else Uk = vel_num(huin, hin);               // h is 0 here: the face kernel's u
-    }
-    double U0h = 0, U0hu = 0, U0hv = 0;
-    if (MODE == 2) { U0h = a.oh[k]; U0hu = a.ohu[k]; U0hv = a.ohv[k]; }
-    const double thC = sm.th[ly + 1][lx + 1];
-    const double rdx = a.m.rdxRow[gj], dxr = a.m.dxRow[gj];
-    double ah = 0, ahu = 0, ahv = 0;
-    if (hasW) {                                       // west face, cell is its right side
-      const double thf = wM >= 0 ? sm.th[ly + 1][lx] : thC;
-      const double inv = thf == 1 ? rdx : thf / dxr;
-      ah += wM * inv; ahu += wN * inv; ahv += wT * inv;
-    }
-    if (hasE) {                                       // east face, cell is its left side
-      const double thf = eM >= 0 ? thC : sm.th[ly + 1][lx + 2];
-      const double inv = thf == 1 ? rdx : thf / dxr;
-      ah -= eM * inv; ahu -= eN * inv; ahv -= eT * inv;
-    }
-    if (hasS) {                                       // south face, cell is its upper side
-      const double thf = sM >= 0 ? sm.th[ly][lx + 1] : thC;
-      const double invR = thf == 1 ? a.m.rdyRowS[gj] : thf / a.m.dyRowS[gj];
-      ah += sM * invR; ahv += sN * invR; ahu += sT * invR;
-    }
-    if (hasN) {                                       // north face, cell is its lower side
-      const double thf = nM >= 0 ? thC : sm.th[ly + 2][lx + 1];
-      const double invL = thf == 1 ? a.m.rdyRowN[gj] : thf / a.m.dyRowN[gj];
-      ah -= nM * invL; ahv -= nN * invL; ahu -= nT * invL;
-    }
-    if (interior) {
-      if (bedOn) {
-        ahu += tb0;
-        ahv += tb1;
-        if (sph) ahv += tg;
-      }
-      if (sph) {
-        const double fe = a.m.fRow[gj] + Uk * (a.m.tanPhi[gj] / a.m.R);
-        ahu += fe * hvin;
-        ahv -= fe * huin;
-      } else if (corOn) {
-        ahu += a.coriolis * hvin;
-        ahv -= a.coriolis * huin;
-      }
-    }
-    if (a.tape_th) a.tape_th[k] = thC;
-    if (MODE == 1) {
-      double nh = hin + dt * ah, nhu = huin + dt * ahu, nhv = hvin + dt * ahv;
-      if (a.tape_hpre) a.tape_hpre[k] = nh;
-      if (interior) {                                 // dryClean, src/swe.mjs:734-745
-        if (nh < 0) { locFl -= nh; nh = 0; }
-        if (nh <= dry) { nhu = 0; nhv = 0; }
-      }
-      a.oh[k] = nh; a.ohu[k] = nhu; a.ohv[k] = nhv;
-    } else {
-      const double h0 = U0h, hu0 = U0hu, hv0 = U0hv;   // U0 (in place)
-      if (a.h0c) { a.h0c[k] = h0; a.hu0c[k] = hu0; a.hv0c[k] = hv0; }
-      double nh = 0.5 * (h0 + hin + dt * ah);
-      double nhu = 0.5 * (hu0 + huin + dt * ahu);
-      double nhv = 0.5 * (hv0 + hvin + dt * ahv);
-      if (a.tape_hpre) a.tape_hpre[k] = nh;
-      if (interior) {
-        if (nh < 0) { locFl -= nh; nh = 0; }
-        if (nh <= dry) { nhu = 0; nhv = 0; }
-        if (a.tape_pre[0]) { a.tape_pre[0][k] = nh; a.tape_pre[1][k] = nhu; a.tape_pre[2][k] = nhv; }
-        // friction, src/swe.mjs:659-704
-        const double n = a.nfield ? a.nfield[k] : a.manning;
-        const bool fricOn = a.nfield ? true : (n != 0 && n == n);
-        if (fricOn) {
-          if (nh <= dry) { nhu = 0; nhv = 0; }
-          else if (n != 0 && n == n) {
-            const double den = vel_den(nh, eps4);
-            const double u = vel_num(nhu, nh) / den, v = vel_num(nhv, nh) / den;
-            const double speed = hypot(u, v);
-            if (!(speed < 1e-14)) {
-              const double denom = 1 + dt * SWE_G * n * n * speed / pow(nh, 4.0 / 3.0);
-              nhu = nhu / denom;
-              nhv = nhv / denom;
-            }
-          }
-        }
-        // sponge, src/swe.mjs:1188-1197
-        if (a.sponge_width > 0) {
-          const int ii = gi - 2, jj = gj - 2;
-          int d;
-          if (a.sponge_side == 1) d = a.nx - 1 - ii; else if (a.sponge_side == 0) d = ii;
-          else if (a.sponge_side == 3) d = a.ny - 1 - jj; else d = jj;
-          if (d < a.sponge_width) {
-            const double f = jmin(1, a.sponge_str[d] * dt * 60);
-            const double target = jmax0(a.sponge_ref - __ldg(a.b + k));
-            nh = nh + (target - nh) * f;
-            nhu = nhu - nhu * f;
-            nhv = nhv - nhv * f;
-          }
-        }
-        // CFL rate of the final state, src/swe.mjs:632-647
-        if (!(nh <= dry)) {
-          const double cc = sqrt(SWE_G * nh);
-          const double den = vel_den(nh, eps4);
-          const double u = fabs(vel_num(nhu, nh) / den), v = fabs(vel_num(nhv, nh) / den);
-          const double sr5 = (u + cc) / dxr + (v + cc) / a.m.dyCFL[gj];
-          if (sr5 > locMax) locMax = sr5;
-        }
-      }
-      a.oh[k] = nh; a.ohu[k] = nhu; a.ohv[k] = nhv;
-    }
+    if (fold) split_cell<MODE, true>(a, s, sm, t, lx, ly, gi, gj, dt, locMax, locFl);
+    else split_cell<MODE, false>(a, s, sm, t, lx, ly, gi, gj, dt, locMax, locFl);
   }
 
-  // per-block partials, then the last block of the grid closes the step
-  for (int o = 16; o > 0; o >>= 1) {
-    locMax = fmax(locMax, __shfl_down_sync(0xffffffffu, locMax, o));
-    locFl += __shfl_down_sync(0xffffffffu, locFl, o);
+  // per-block partials, then the last block of the grid closes the step.
+  // When no cell contributed (both start at +0 and only change to nonzero
+  // values), the reduction would give +0 and 0: those are written directly.
+  const bool any = __syncthreads_or(locMax != 0 || locFl != 0);   // uniform
+  if (any) {
+    for (int o = 16; o > 0; o >>= 1) {
+      locMax = fmax(locMax, __shfl_down_sync(0xffffffffu, locMax, o));
+      locFl += __shfl_down_sync(0xffffffffu, locFl, o);
+    }
+    if ((t & 31) == 0) { sm.red[0][t >> 5] = locMax; sm.red[1][t >> 5] = locFl; }
+    __syncthreads();
   }
-  if ((t & 31) == 0) { sm.red[0][t >> 5] = locMax; sm.red[1][t >> 5] = locFl; }
-  __syncthreads();
   if (t == 0) {
-    double m = sm.red[0][0], f = sm.red[1][0];
-    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, sm.red[0][w]); f += sm.red[1][w]; }
+    double m = 0, f = 0;
+    if (any) {
+      m = sm.red[0][0]; f = sm.red[1][0];
+      for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, sm.red[0][w]); f += sm.red[1][w]; }
+    }
     if (MODE == 1) a.part_fl1[part] = f;
     else { a.part_max[part] = m; a.part_fl2[part] = f; }
     if (ticket) {
