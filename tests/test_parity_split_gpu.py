@@ -48,3 +48,46 @@ def test_tiled_and_fused_give_the_same_bits(swe, case, monkeypatch):
     for a, b in zip(out["fused"][:3], out["split"][:3]):
         assert np.array_equal(a, b)
     assert out["fused"][3] == out["split"][3]
+
+
+def test_dry_tile_flags_follow_host_writes(swe, monkeypatch):
+    """The cell kernel records which tiles it left with h == 0 everywhere,
+    and the next face kernel skips tiles whose 3 x 3 neighbourhood is so
+    recorded.  Every other writer of the state clears those records: water
+    poured onto dry land by the host, dryClean, friction, and a switch to
+    the fused kernels and back.  Through all of them the tiled pair stays
+    bit-identical (uint64 patterns) to the fused kernel."""
+    import ctypes
+    import numpy as np
+    from water_simulator_b200 import workloads
+    lib = swe.load_library()
+
+    def scenario(impl):
+        monkeypatch.setenv("SWE_B200_STAGE", impl)
+        b, h = workloads.beach_dam_break(nx=256, ny=96, dx=8.0)
+        sim = swe.ShallowWater(nx=256, ny=96, dx=8.0, bed=b, eta0=b + h, manning=0.03)
+        sim.boundaries = {"west": swe.flather(lambda t: 0.0, lambda t: 0.0)}
+        assert sim.run(40) == 40
+        hh = np.array(sim.field("h")).reshape(sim.H, sim.W)
+        assert (hh[30:70, 160:240] == 0).all()            # dry land, tiles deep inside it
+        hh[40:60, 170:230] += 0.7                         # a pond poured onto it
+        sim.h = hh.reshape(-1)
+        assert sim.run(30) == 30
+        sim.dryClean()
+        assert sim.run(10) == 10
+        sim.applyFriction(sim.maxDt())
+        assert sim.run(10) == 10
+        other = 0 if impl == "split" else 1               # there and back
+        mine = 1 - other
+        swe._lib.check(lib.swe_set_stage_kernels(sim._h, other))
+        assert sim.run(5) == 5
+        swe._lib.check(lib.swe_set_stage_kernels(sim._h, mine))
+        assert sim.run(25) == 25
+        out = [sim.field(f).view(np.uint64).copy() for f in ("h", "hu", "hv")] + [sim.t]
+        sim.close()
+        return out
+
+    fused, split = scenario("fused"), scenario("split")
+    for a, b in zip(fused[:3], split[:3]):
+        assert np.array_equal(a, b)
+    assert fused[3] == split[3]

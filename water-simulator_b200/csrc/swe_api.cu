@@ -92,6 +92,7 @@ struct swe_sim {
   // stage kernels: 0 the fused row-marching kernel, 1 the two tiled kernels
   int stage_impl = 0;
   double* d_split = nullptr;
+  int* d_odry[2] = {nullptr, nullptr};             // per tile of A / B: all h == 0 (swe_split.cuh)
   swe::SplitBufs sb;
   dim3 sgrid;
   cudaGraphExec_t gexec = nullptr;
@@ -99,6 +100,17 @@ struct swe_sim {
   double g_dt = 0, g_tend = 0;
   unsigned long long g_version = 0, version = 1;
 };
+
+namespace {
+// The state was written outside a stage: no tile is known dry any more.
+int forget_dry(swe_sim* s) {
+  if (!s->d_odry[0]) return SWE_OK;
+  const size_t bytes = sizeof(int) * (size_t)s->sgrid.x * s->sgrid.y;
+  CU(cudaMemsetAsync(s->d_odry[0], 0, bytes, s->st));
+  CU(cudaMemsetAsync(s->d_odry[1], 0, bytes, s->st));
+  return SWE_OK;
+}
+}  // namespace
 
 namespace swe_host {
 cudaStream_t stream_of(swe_sim* s) { return s->st; }
@@ -116,6 +128,7 @@ int adopt_fields(swe_sim* s, const double* d_b, const double* d_h, const double*
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
   if (e != cudaSuccess) { set_error(std::string("adopt_fields: ") + cudaGetErrorString(e)); return SWE_ECUDA; }
+  if (forget_dry(s)) return SWE_ECUDA;
   s->version++;
   s->cfl_valid = false;
   return SWE_OK;
@@ -277,22 +290,28 @@ int ensure_split(swe_sim* s) {
   if (s->d_split) return SWE_OK;
   const size_t N = s->N;
   const size_t ntiles = (size_t)s->sgrid.x * s->sgrid.y;
-  const size_t doubles = swe::SPLIT_FIELDS * N + (ntiles + 1) / 2;       // + one int flag per tile
+  const size_t doubles = swe::SPLIT_FIELDS * N + 3 * ((ntiles + 1) / 2);   // + three int flags per tile
   CU(cudaMalloc(&s->d_split, sizeof(double) * doubles));
   CU(cudaMemsetAsync(s->d_split, 0, sizeof(double) * doubles, s->st));
   s->sb = swe::split_bufs_at(s->d_split, N);
   s->sb.dry = reinterpret_cast<int*>(s->d_split + swe::SPLIT_FIELDS * N);
   s->sb.ntx = (int)s->sgrid.x;
   s->sb.nty = (int)s->sgrid.y;
+  s->d_odry[0] = reinterpret_cast<int*>(s->d_split + swe::SPLIT_FIELDS * N + (ntiles + 1) / 2);
+  s->d_odry[1] = reinterpret_cast<int*>(s->d_split + swe::SPLIT_FIELDS * N + 2 * ((ntiles + 1) / 2));
   return SWE_OK;
 }
+
 
 // One stage (MODE 1 or 2) with the selected kernels.
 template <int MODE>
 int launch_stage(swe_sim* s, const swe::StageArgs& a) {
   if (s->stage_impl == 1) {
-    swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, s->sb, s->d_ctl);
-    swe::k_split_cells<MODE><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, s->sb, s->d_ctl);
+    swe::SplitBufs sb = s->sb;                      // stage 1: A -> B, stage 2: B -> A
+    sb.odry_in = s->d_odry[MODE == 1 ? 0 : 1];
+    sb.odry_out = s->d_odry[MODE == 1 ? 1 : 0];
+    swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, sb, s->d_ctl);
+    swe::k_split_cells<MODE><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, sb, s->d_ctl);
     swe::k_split_close<MODE><<<1, swe::SP_THREADS, 0, s->st>>>(a, s->d_ctl, (int)(s->sgrid.x * s->sgrid.y));
   } else {
     swe::k_stage<MODE><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a, s->d_ctl);
@@ -548,6 +567,7 @@ int swe_set_field(swe_sim* s, int field, const double* in) {
     return fail(SWE_EINVAL, "only b, h, hu, hv are writable (use swe_set_manning_field for n)");
   const size_t nb = sizeof(double) * (size_t)s->N;
   CU(cudaMemcpyAsync(field_ptr(s, field), in, nb, cudaMemcpyHostToDevice, s->st));
+  if (field != SWE_FIELD_B && forget_dry(s)) return SWE_ECUDA;
   s->cfl_valid = false;
   return SWE_OK;
 }
@@ -748,6 +768,7 @@ int swe_apply_friction(swe_sim* s, double dt) {
   swe::StageArgs a = stage_args(s, s->d_A, s->d_A);
   swe::k_friction<<<std::max(1, std::min(4096, (s->nx * s->ny + 255) / 256)), 256, 0, s->st>>>(a, dt);
   CU(cudaGetLastError());
+  if (forget_dry(s)) return SWE_ECUDA;
   CU(cudaStreamSynchronize(s->st));
   s->cfl_valid = false;
   return SWE_OK;
@@ -758,6 +779,7 @@ int swe_dry_clean(swe_sim* s, double* added) {
   swe::StageArgs a = stage_args(s, s->d_A, s->d_A);
   swe::k_dry_clean<<<1, 1, 0, s->st>>>(a, s->d_ctl);
   CU(cudaGetLastError());
+  if (forget_dry(s)) return SWE_ECUDA;
   swe::Control c;
   const int rc = read_ctl(s, &c);
   if (rc) return rc;
@@ -985,6 +1007,8 @@ int swe_set_stage_kernels(swe_sim* s, int impl) {
     int rc = ensure_split(s);
     if (rc) return rc;
   }
+  // the fused kernels write no dry flags: whatever a switch leaves is stale
+  if (forget_dry(s)) return SWE_ECUDA;
   s->stage_impl = impl;
   s->version++;                     // the cached graph holds the other kernels
   return SWE_OK;

@@ -65,6 +65,13 @@ struct SplitBufs {
   double* V;
   int* dry;                        // per tile: 1 when its faces were not written (dry), or null
   int ntx, nty;                    // tiles per row and column of the grid
+  // optional, per tile of the stage's input / output state: 1 when every
+  // cell of the tile has h exactly 0 and none is a ghost cell (so nothing
+  // but a stage or the host writes it).  The cell kernel writes odry_out
+  // with the state; the face kernel reads odry_in.  Whoever else writes the
+  // state clears them.
+  const int* odry_in;
+  int* odry_out;
 };
 
 // The SPLIT_FIELDS fields of one grid, `stride` doubles apart from `base`.
@@ -80,6 +87,8 @@ __host__ __forceinline__ SplitBufs split_bufs_at(double* base, size_t stride) {
   b.V = nullptr;
   b.dry = nullptr;
   b.ntx = b.nty = 0;
+  b.odry_in = nullptr;
+  b.odry_out = nullptr;
   return b;
 }
 
@@ -171,6 +180,20 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
   const bool sph = a.sph != 0;
   const bool bedOn = order2 || sph;
   const int t = threadIdx.x;
+
+  // A tile whose 3 x 3 neighbourhood of tiles holds only h == 0 (outside
+  // the grid counts as zero state) is dry with its halo: nothing to load.
+  if (s.odry_in && s.dry && !s.sl[0]) {
+    int f = 1;
+    if (t < 9) {
+      const int r = t / 3, c = t - 3 * r, txn = tx - 1 + c, tyn = ty - 1 + r;
+      if (txn >= 0 && txn < s.ntx && tyn >= 0 && tyn < s.nty) f = s.odry_in[tyn * s.ntx + txn];
+    }
+    if (__syncthreads_and(f)) {                   // uniform across the CTA
+      if (t == 0) s.dry[ty * s.ntx + tx] = 1;
+      return;
+    }
+  }
 
   // state of the tile and its halo (zero outside the grid): b, h, hu, hv
   // copied into b, h, U, V with every copy of the thread in flight at once;
@@ -379,7 +402,7 @@ __device__ __forceinline__ void split_close_block(const StageArgs& a, Control* c
 template <int MODE, bool DRY>
 __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& s, const CellsSmem& sm, int t,
                                            int lx, int ly, int gi, int gj, double dt, double& locMax,
-                                           double& locFl) {
+                                           double& locFl, double& hout) {
   const int W = a.W, H = a.H;
   const double dry = a.minDepth, eps4 = a.eps4;
   const bool sph = a.sph != 0;
@@ -453,6 +476,7 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
       if (nh < 0) { locFl -= nh; nh = 0; }
       if (nh <= dry) { nhu = 0; nhv = 0; }
     }
+    hout = nh;
     a.oh[k] = nh; a.ohu[k] = nhu; a.ohv[k] = nhv;
   } else {
     const double h0 = U0h, hu0 = U0hu, hv0 = U0hv;   // U0 (in place)
@@ -504,6 +528,7 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
         if (sr5 > locMax) locMax = sr5;
       }
     }
+    hout = nh;
     a.oh[k] = nh; a.ohu[k] = nhu; a.ohv[k] = nhv;
   }
 }
@@ -558,10 +583,15 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
     __syncthreads();
   }
 
-  double locMax = 0, locFl = 0;
+  double locMax = 0, locFl = 0, hout = 0;
   if (gi < W && gj < H) {
-    if (fold) split_cell<MODE, true>(a, s, sm, t, lx, ly, gi, gj, dt, locMax, locFl);
-    else split_cell<MODE, false>(a, s, sm, t, lx, ly, gi, gj, dt, locMax, locFl);
+    if (fold) split_cell<MODE, true>(a, s, sm, t, lx, ly, gi, gj, dt, locMax, locFl, hout);
+    else split_cell<MODE, false>(a, s, sm, t, lx, ly, gi, gj, dt, locMax, locFl, hout);
+  }
+  if (s.odry_out) {                               // the written tile's flag
+    const bool ghostFree = i0 >= 2 && i0 + SPX <= W - 2 && j0 >= 2 && j0 + SPY <= H - 2;
+    const bool own = __syncthreads_and(hout == 0) && ghostFree;
+    if (t == 0) s.odry_out[ty * s.ntx + tx] = own ? 1 : 0;
   }
 
   // per-block partials, then the last block of the grid closes the step.
