@@ -91,6 +91,7 @@ struct swe_sim {
   // device-resident loop graph
   // stage kernels: 0 the fused row-marching kernel, 1 the two tiled kernels
   int stage_impl = 0;
+  int pdl = 1;                                     // programmatic dependent launch in the stepping loop
   double* d_split = nullptr;
   int* d_odry[2] = {nullptr, nullptr};             // per tile of A / B: all h == 0 (swe_split.cuh)
   swe::SplitBufs sb;
@@ -278,9 +279,26 @@ swe::PrepArgs prep_args(const swe_sim* s, int mode, double dt, double t_end) {
 
 int bc_blocks(const swe_sim* s) { return (4 * s->ny + 4 * (s->nx + 4) + 255) / 256; }
 
-int launch_bc(swe_sim* s, double* const* f, int respect_stop) {
-  swe::k_apply_bc<<<bc_blocks(s), 256, 0, s->st>>>(bc_args(s, f), s->d_ctl, respect_stop);
-  CU(cudaGetLastError());
+// A launch that, with `pdl`, may be scheduled before the previous kernel in
+// the stream has finished (the kernel waits for it in pdl_enter).
+template <typename... KArgs, typename... Args>
+cudaError_t launch(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+int launch_bc(swe_sim* s, double* const* f, int respect_stop, bool pdl = false) {
+  CU(launch(pdl, swe::k_apply_bc, dim3(bc_blocks(s)), dim3(256), s->st, bc_args(s, f),
+            (const swe::Control*)s->d_ctl, respect_stop));
   return SWE_OK;
 }
 
@@ -305,14 +323,15 @@ int ensure_split(swe_sim* s) {
 
 // One stage (MODE 1 or 2) with the selected kernels.
 template <int MODE>
-int launch_stage(swe_sim* s, const swe::StageArgs& a) {
+int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
   if (s->stage_impl == 1) {
     swe::SplitBufs sb = s->sb;                      // stage 1: A -> B, stage 2: B -> A
     sb.odry_in = s->d_odry[MODE == 1 ? 0 : 1];
     sb.odry_out = s->d_odry[MODE == 1 ? 1 : 0];
-    swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, sb, s->d_ctl);
-    swe::k_split_cells<MODE><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a, sb, s->d_ctl);
-    swe::k_split_close<MODE><<<1, swe::SP_THREADS, 0, s->st>>>(a, s->d_ctl, (int)(s->sgrid.x * s->sgrid.y));
+    const dim3 blk(swe::SP_THREADS);
+    CU(launch(pdl, swe::k_split_faces, s->sgrid, blk, s->st, a, sb, s->d_ctl));
+    CU(launch(pdl, swe::k_split_cells<MODE>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
+    CU(launch(pdl, swe::k_split_close<MODE>, dim3(1), blk, s->st, a, s->d_ctl, (int)(s->sgrid.x * s->sgrid.y)));
   } else {
     swe::k_stage<MODE><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a, s->d_ctl);
   }
@@ -321,21 +340,23 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a) {
 }
 
 int enqueue_step(swe_sim* s, int mode, double dt, double t_end) {
-  swe::k_prepare<<<1, 32, 0, s->st>>>(s->d_ctl, prep_args(s, mode, dt, t_end));
-  CU(cudaGetLastError());
+  // The tiled kernels, the ghost fills and prepare enter through pdl_enter,
+  // so each may be scheduled while its predecessor drains.
+  const bool pdl = s->pdl && s->stage_impl == 1;
+  CU(launch(pdl, swe::k_prepare, dim3(1), dim3(32), s->st, s->d_ctl, prep_args(s, mode, dt, t_end)));
   // Host-checked dt (mode 0) never reaches here refused.  In the device loop
   // a refused step (t reached t_end) changes nothing, ghosts included, as the
   // drivers' `while (sim.t < T)` loop stops calling step().
-  int rc = launch_bc(s, s->d_A, mode == 0 ? 0 : 1);
+  int rc = launch_bc(s, s->d_A, mode == 0 ? 0 : 1, pdl);
   if (rc) return rc;
   swe::StageArgs a1 = stage_args(s, s->d_A, s->d_B);
-  rc = launch_stage<1>(s, a1);
+  rc = launch_stage<1>(s, a1, pdl);
   if (rc) return rc;
-  rc = launch_bc(s, s->d_B, 1);
+  rc = launch_bc(s, s->d_B, 1, pdl);
   if (rc) return rc;
   swe::StageArgs a2 = stage_args(s, s->d_B, s->d_A);
   if (s->keep_h0) { a2.h0c = s->d_h0[0]; a2.hu0c = s->d_h0[1]; a2.hv0c = s->d_h0[2]; }
-  return launch_stage<2>(s, a2);
+  return launch_stage<2>(s, a2, pdl);
 }
 
 int ensure_cfl(swe_sim* s) {
@@ -524,6 +545,8 @@ int swe_create(const swe_options* o, const double* b, const double* h, swe_sim**
     s->stage_impl = (env && std::strcmp(env, "fused") == 0) ? 0 : (env && std::strcmp(env, "split") == 0) ? 1
                                                                   : SWE_DEFAULT_STAGE;
     if (s->stage_impl == 1 && ensure_split(s)) return bail(SWE_ECUDA);
+    const char* pe = std::getenv("SWE_B200_PDL");
+    s->pdl = (pe && std::strcmp(pe, "0") == 0) ? 0 : 1;
   }
   CUB(cudaStreamSynchronize(s->st));
 #undef CUB

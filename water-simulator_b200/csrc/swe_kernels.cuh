@@ -139,7 +139,18 @@ __device__ __forceinline__ void prepare_one(Control* ctl, const PrepArgs& a) {
   }
 }
 
+// Programmatic dependent launch (sm_90+).  A kernel of the stepping loop
+// lets the next one be scheduled as soon as all of its own CTAs have
+// started, then waits until every grid it depends on has finished and its
+// writes are visible, before it reads or writes anything.  Launched without
+// the programmatic attribute, both are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+
 __global__ void k_prepare(Control* ctl, PrepArgs a) {
+  pdl_enter();
   if (threadIdx.x == 0) prepare_one(ctl, a);
 }
 
@@ -257,6 +268,7 @@ __device__ __forceinline__ void apply_bc_range(const BCArgs& a, const Control* c
 }
 
 __global__ void k_apply_bc(BCArgs a, const Control* ctl, int respect_stop) {
+  pdl_enter();
   if (respect_stop && ctl->stop) return;
   apply_bc_range(a, ctl, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }

@@ -291,6 +291,7 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
 #endif
 __global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_FACES_MIN_BLOCKS)
 k_split_faces(StageArgs a, SplitBufs s, Control* ctl) {
+  pdl_enter();
   if (ctl->stop) return;
   __shared__ FacesSmem sm;
   split_faces_tile(a, s, blockIdx.x, blockIdx.y, sm);
@@ -633,6 +634,7 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
 template <int MODE>
 __global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_CELLS_MIN_BLOCKS)
 k_split_cells(StageArgs a, SplitBufs s, Control* ctl) {
+  pdl_enter();
   if (ctl->stop) return;
   __shared__ CellsSmem sm;
   split_cells_tile<MODE>(a, s, ctl, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
@@ -643,6 +645,7 @@ k_split_cells(StageArgs a, SplitBufs s, Control* ctl) {
 // ticket shared by every tile of a large grid serialises in L2).
 template <int MODE>
 __global__ void __launch_bounds__(SP_THREADS) k_split_close(StageArgs a, Control* ctl, int nparts) {
+  pdl_enter();
   if (ctl->stop) return;
   __shared__ CellsSmem sm;
   split_close_block<MODE>(a, ctl, nparts, sm);
