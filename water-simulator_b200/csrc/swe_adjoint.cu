@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <unordered_map>
@@ -39,6 +40,7 @@ using swe::BCArgs;
 using swe::Control;
 using swe::adj::FaceIn;
 using swe::StageArgs;
+using swe::pdl_enter;
 
 int fail(int code, const std::string& m) { swe_host::set_error(m); return code; }
 
@@ -80,9 +82,6 @@ __device__ __forceinline__ FaceIn yface_in(const Geo& g, const double* b, const 
 // ---- adjoint of the residual -------------------------------------------------
 struct AdjBuf {
   double *lR[3];          // adjoints of rh, rhu, rhv (input)
-  double *gx[16], *gy[16];// face-input adjoints (FaceIn order)
-  double *gs[16];         // per cell: (dslope/da, dslope/dc) x adjoint, 8 slopes
-  double *dir[4];         // per cell: direct adjoints of b, h, U, V
 };
 
 // Face accumulation (src/swe.mjs:530-555) backwards, one face at a time:
@@ -161,163 +160,278 @@ __device__ __forceinline__ double lout_of(const Geo& g, const Inter& it, const d
   return lo;
 }
 
-// The faces backwards: limiter terms into the flux adjoint, then
-// face_flux's reverse.
-// 128 registers at most: 16 warps per SM instead of the 8 that 140 leave.
-constexpr int FACES_CORE_THREADS = 128;
-#ifndef SWE_FACES_CORE_MIN_BLOCKS
-#define SWE_FACES_CORE_MIN_BLOCKS 4
+// ---- the residual backwards on 32-column tiles ---------------------------------
+// The face kernels hand each cell the sum of its two faces' adjoints in one
+// direction (8 values) instead of each face's 16, and the cell kernel runs
+// the cell gather and the slopes' neighbour gather in one pass over a tile
+// with a one-cell ring, so neither the per-face halves nor the slope
+// derivatives go through device memory.
+//
+// x faces: a warp is 32 consecutive cells of a row (tile column bx).  Lane
+// t's face is (i | i+1); its right half belongs to lane t+1 (a shuffle),
+// lane 31's to lane 0 of tile bx+1 (the edge buffer ex, indexed (j, bx)).
+// y faces: a 32 x 8 tile; row ty's upper half goes to row ty+1 through
+// shared memory, row 7's to row 0 of tile row by+1 (ey, indexed (by, i)).
+// Per-cell sums are in FaceIn's left-side order: b, h, normal, transverse,
+// sE, sB, s(normal), s(transverse).
+constexpr int AT_X = 32;           // tile width (one warp)
+constexpr int AT_XROWS = 4;        // rows per x-face block (128 threads)
+constexpr int AT_Y = 8;            // rows per y-face / cell tile (256 threads)
+// The face kernels are latency bound: capped at 64 registers (32 warps per
+// SM; a few hundred bytes of spills) they measured faster than at 80
+// (24 warps) or at their natural 112 (16 warps).
+#ifndef SWE_ADJ_FACE_WARPS
+#define SWE_ADJ_FACE_WARPS 32
 #endif
-// One launch for the x faces and one for the y faces: one face per thread
-// fits 128 registers without spilling (16 warps per SM) and measured
-// faster than both faces per thread at 128 or 168 registers.
-#ifndef SWE_FACES_CORE_SPLIT
-#define SWE_FACES_CORE_SPLIT 1
+// The cell kernel waits on memory: four blocks per SM (64 registers,
+// 32 warps) instead of the three its natural 80 registers leave.
+#ifndef SWE_ADJ_CELL_BLOCKS
+#define SWE_ADJ_CELL_BLOCKS 4
 #endif
-// WHICH: 0 the x face of each cell, 1 its y face, 2 both.
-template <int WHICH>
-__global__ void __launch_bounds__(FACES_CORE_THREADS, SWE_FACES_CORE_MIN_BLOCKS)
-k_adj_faces_core(Geo g, const double* b, const double* h, Inter it, const double* theta, double dt, AdjBuf a) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
-    const int i = k % g.W, j = k / g.W;
-    if (WHICH != 1) {
-      FaceIn gx = {};
-      if (xface_on(g, i, j)) {
-        const FaceAdj f = xface_adj(g, it, theta, a, k, i, j);
-        double lM = f.lM;
-        const double M = it.fx[F_M][k];
-        if (M > 0) lM += lout_of(g, it, theta, h, dt, a, k) / g.dxRow[j];
-        if (M < 0) lM -= lout_of(g, it, theta, h, dt, a, k + 1) / g.dxRow[j];
-        gx = swe::adj::face_rev(xface_in(g, b, h, it, k), g.minDepth, lM, f.lN, f.lT, f.lpL, f.lpR);
-      }
-      const double* px = &gx.bL;
-      for (int q = 0; q < 16; q++) a.gx[q][k] = px[q];
-    }
-    if (WHICH != 0) {
-      FaceIn gy = {};
-      if (yface_on(g, i, j)) {
-        const FaceAdj f = yface_adj(g, it, theta, a, k, i, j);
-        double lM = f.lM;
-        const double M = it.fy[F_M][k];
-        if (M > 0) lM += lout_of(g, it, theta, h, dt, a, k) / g.dyRowN[j];
-        if (M < 0) lM -= lout_of(g, it, theta, h, dt, a, k + g.W) / g.dyRowS[j + 1];
-        gy = swe::adj::face_rev(yface_in(g, b, h, it, k), g.minDepth, lM, f.lN, f.lT, f.lpL, f.lpR);
-      }
-      const double* py = &gy.bL;
-      for (int q = 0; q < 16; q++) a.gy[q][k] = py[q];
-    }
+
+struct FaceSums {
+  double *sx[8], *sy[8];           // per cell: its east + west x faces, its north + south y faces
+  double *ex[8], *ey[8];           // halves that cross a tile edge
+  int ntx;                         // tiles per row (ceil(W / 32))
+};
+
+__global__ void __launch_bounds__(AT_X * AT_XROWS, SWE_ADJ_FACE_WARPS / AT_XROWS)
+k_adj_xfaces(Geo g, const double* b, const double* h, Inter it, const double* theta, double dt, AdjBuf a,
+             FaceSums S) {
+  pdl_enter();
+  const int tx = threadIdx.x, bx = blockIdx.x;
+  const int i = bx * AT_X + tx, j = blockIdx.y * AT_XROWS + threadIdx.y;
+  const bool valid = i < g.W && j < g.H;
+  const int k = j * g.W + i;
+  FaceIn gx = {};
+  if (valid && xface_on(g, i, j)) {
+    const FaceAdj f = xface_adj(g, it, theta, a, k, i, j);
+    double lM = f.lM;
+    const double M = it.fx[F_M][k];
+    if (M > 0) lM += lout_of(g, it, theta, h, dt, a, k) / g.dxRow[j];
+    if (M < 0) lM -= lout_of(g, it, theta, h, dt, a, k + 1) / g.dxRow[j];
+    gx = swe::adj::face_rev(xface_in(g, b, h, it, k), g.minDepth, lM, f.lN, f.lT, f.lpL, f.lpR);
+  }
+  const double* p = &gx.bL;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const double r = __shfl_up_sync(0xffffffffu, p[8 + q], 1);
+    if (valid) S.sx[q][k] = tx > 0 ? p[q] + r : p[q];
+  }
+  if (tx == AT_X - 1 && j < g.H) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) S.ex[q][(size_t)j * S.ntx + bx] = p[8 + q];
   }
 }
 
-enum { F_BL, F_HL, F_NL, F_TL, F_SEL, F_SBL, F_SNL, F_STL, F_BR, F_HR, F_NR, F_TR, F_SER, F_SBR, F_SNR, F_STR };
+__global__ void __launch_bounds__(AT_X * AT_Y, SWE_ADJ_FACE_WARPS / AT_Y)
+k_adj_yfaces(Geo g, const double* b, const double* h, Inter it, const double* theta, double dt, AdjBuf a,
+             FaceSums S) {
+  pdl_enter();
+  __shared__ double up[AT_Y][8][AT_X];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.x * AT_X + tx, j = blockIdx.y * AT_Y + ty;
+  const bool valid = i < g.W && j < g.H;
+  const int k = j * g.W + i;
+  FaceIn gy = {};
+  if (valid && yface_on(g, i, j)) {
+    const FaceAdj f = yface_adj(g, it, theta, a, k, i, j);
+    double lM = f.lM;
+    const double M = it.fy[F_M][k];
+    if (M > 0) lM += lout_of(g, it, theta, h, dt, a, k) / g.dyRowN[j];
+    if (M < 0) lM -= lout_of(g, it, theta, h, dt, a, k + g.W) / g.dyRowS[j + 1];
+    gy = swe::adj::face_rev(yface_in(g, b, h, it, k), g.minDepth, lM, f.lN, f.lT, f.lpL, f.lpR);
+  }
+  const double* p = &gy.bL;
+#pragma unroll
+  for (int q = 0; q < 8; q++) up[ty][q][tx] = p[8 + q];
+  __syncthreads();
+  if (valid) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) S.sy[q][k] = ty > 0 ? p[q] + up[ty - 1][q][tx] : p[q];
+  }
+  if (ty == AT_Y - 1 && i < g.W) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) S.ey[q][(size_t)blockIdx.y * g.W + i] = p[8 + q];
+  }
+}
 
-// Per cell: gather the faces' adjoints, add the bed term and Coriolis
-// backwards, then the limiter derivatives of each slope.
-__global__ void k_adj_cells(Geo g, const double* b, const double* h, const double* hu, const double* hv,
-                            Inter it, const double* theta, double dt, AdjBuf a, double* lhu, double* lhv) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
-    const int i = k % g.W, j = k / g.W;
-    double db = 0, dh = 0, dU = 0, dV = 0;
-    double ls[8] = {0, 0, 0, 0, 0, 0, 0, 0};         // sE0 sB0 sU0 sV0 sE1 sB1 sU1 sV1
-    if (i + 1 < g.W && xface_on(g, i, j)) {          // east x face, cell is its left side
-      db += a.gx[F_BL][k]; dh += a.gx[F_HL][k]; dU += a.gx[F_NL][k]; dV += a.gx[F_TL][k];
-      ls[0] += a.gx[F_SEL][k]; ls[1] += a.gx[F_SBL][k]; ls[2] += a.gx[F_SNL][k]; ls[3] += a.gx[F_STL][k];
+// The face sums of cell (i, j) in direction d (0: x, 1: y), with the half
+// that crossed a tile edge: b, h, U, V and the four slope adjoints of that
+// direction (sE, sB, sU, sV).
+__device__ __forceinline__ void face_sums(const Geo& g, const FaceSums& S, int d, int i, int j, int k,
+                                          double& db, double& dh, double& dU, double& dV, double ls[4]) {
+  double v[8];
+  if (d == 0) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = S.sx[q][k];
+    if ((i & (AT_X - 1)) == 0 && i >= AT_X) {
+      const size_t e = (size_t)j * S.ntx + (i / AT_X - 1);
+#pragma unroll
+      for (int q = 0; q < 8; q++) v[q] += S.ex[q][e];
     }
-    if (i >= 1 && xface_on(g, i - 1, j)) {           // west x face, cell is its right side
-      const int f = k - 1;
-      db += a.gx[F_BR][f]; dh += a.gx[F_HR][f]; dU += a.gx[F_NR][f]; dV += a.gx[F_TR][f];
-      ls[0] += a.gx[F_SER][f]; ls[1] += a.gx[F_SBR][f]; ls[2] += a.gx[F_SNR][f]; ls[3] += a.gx[F_STR][f];
+    db = v[0]; dh = v[1]; dU = v[2]; dV = v[3];
+    ls[0] = v[4]; ls[1] = v[5]; ls[2] = v[6]; ls[3] = v[7];
+  } else {
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = S.sy[q][k];
+    if ((j % AT_Y) == 0 && j >= AT_Y) {
+      const size_t e = (size_t)(j / AT_Y - 1) * g.W + i;
+#pragma unroll
+      for (int q = 0; q < 8; q++) v[q] += S.ey[q][e];
     }
-    if (yface_on(g, i, j)) {                         // north y face, cell is its lower side (v normal)
-      db += a.gy[F_BL][k]; dh += a.gy[F_HL][k]; dV += a.gy[F_NL][k]; dU += a.gy[F_TL][k];
-      ls[4] += a.gy[F_SEL][k]; ls[5] += a.gy[F_SBL][k]; ls[7] += a.gy[F_SNL][k]; ls[6] += a.gy[F_STL][k];
-    }
-    if (j >= 1 && yface_on(g, i, j - 1)) {           // south y face, cell is its upper side
-      const int f = k - g.W;
-      db += a.gy[F_BR][f]; dh += a.gy[F_HR][f]; dV += a.gy[F_NR][f]; dU += a.gy[F_TR][f];
-      ls[4] += a.gy[F_SER][f]; ls[5] += a.gy[F_SBR][f]; ls[7] += a.gy[F_SNR][f]; ls[6] += a.gy[F_STR][f];
-    }
+    // y faces: normal = V, transverse = U; slopes sE1 sB1 sV1 sU1
+    db = v[0]; dh = v[1]; dV = v[2]; dU = v[3];
+    ls[0] = v[4]; ls[1] = v[5]; ls[3] = v[6]; ls[2] = v[7];
+  }
+}
+
+// The bed term of direction d backwards (src/swe.mjs:570-598, Cartesian),
+// into the slope adjoints of that direction and the cell's b, h adjoints.
+__device__ __forceinline__ void bed_term_adj(const Geo& g, const double* b, const double* h, const Inter& it,
+                                             const AdjBuf& a, int d, int j, int k, double ls[4], double& db,
+                                             double& dh) {
+  const double bk = b[k], eC = bk + h[k];
+  const double sE = it.s[4 * d][k], sB = it.s[4 * d + 1][k];
+  const double aP = eC + 0.5 * sE - (bk + 0.5 * sB), aM = eC - 0.5 * sE - (bk - 0.5 * sB);
+  const double hP = swe::jmax0(aP), hM = swe::jmax0(aM);
+  const double div = d == 0 ? g.dxRow[j] : g.bedPhi[j];
+  const double lterm = a.lR[1 + d][k];
+  const double lhPM = lterm * (-SWE_G * 0.5 * sB / div);
+  const double ldb = lterm * (-SWE_G * 0.5 * (hP + hM)) / div;
+  double leC = 0;
+  if (aP > 0) { leC += lhPM; ls[0] += 0.5 * lhPM; db -= lhPM; ls[1] -= 0.5 * lhPM; }
+  if (aM > 0) { leC += lhPM; ls[0] -= 0.5 * lhPM; db -= lhPM; ls[1] += 0.5 * lhPM; }
+  ls[1] += ldb;
+  db += leC; dh += leC;
+}
+
+// The limiter's derivatives for the four slopes of direction d at cell
+// (i, j): ga (with respect to X[k] - X[km]) and gc (X[kp] - X[k]), each
+// times the slope's adjoint.
+__device__ __forceinline__ void limiter_adj(const Geo& g, const double* b, const double* h, const Inter& it, int d,
+                                            int i, int j, int k, const double ls[4], double ga[4], double gc[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) { ga[q] = 0; gc[q] = 0; }
+  if (!(g.order >= 2 && i >= 1 && i < g.W - 1 && j >= 1 && j < g.H - 1)) return;
+  const int kp = d == 0 ? k + 1 : k + g.W, km = d == 0 ? k - 1 : k - g.W;
+  if (h[k] <= g.minDepth || h[kp] <= g.minDepth || h[km] <= g.minDepth) return;
+  const double eC = b[k] + h[k], eP = b[kp] + h[kp], eM = b[km] + h[km];
+  const double X0[4] = {eC - eM, b[k] - b[km], it.U[k] - it.U[km], it.V[k] - it.V[km]};
+  const double X1[4] = {eP - eC, b[kp] - b[k], it.U[kp] - it.U[k], it.V[kp] - it.V[k]};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    double da, dc;
+    swe::adj::limiter_grad(g.lim, X0[q], X1[q], da, dc);
+    ga[q] = ls[q] * da;
+    gc[q] = ls[q] * dc;
+  }
+}
+
+// The slope adjoints of direction d at a cell, as its own tile computes
+// them: face sums, plus the bed term on interior cells.
+__device__ __forceinline__ void dir_slopes(const Geo& g, const double* b, const double* h, const Inter& it,
+                                           const AdjBuf& a, const FaceSums& S, int d, int i, int j, int k,
+                                           double ls[4], double& db, double& dh, double& dU, double& dV) {
+  face_sums(g, S, d, i, j, k, db, dh, dU, dV, ls);
+  const bool interior = i >= 2 && i < g.W - 2 && j >= 2 && j < g.H - 2;
+  if (interior && g.order >= 2) bed_term_adj(g, b, h, it, a, d, j, k, ls, db, dh);
+}
+
+// Per cell of a 32 x 8 tile: gather the face sums, the bed term and
+// Coriolis backwards, the positivity limiter's depth adjoint, the limiter
+// derivatives of the slopes; then each cell collects the slope derivatives
+// that land on it from itself and its four neighbours (the ring cells'
+// derivatives are formed by this block too), and the velocities' reverse.
+__global__ void __launch_bounds__(AT_X * AT_Y, SWE_ADJ_CELL_BLOCKS)
+k_adj_cells_tiled(Geo g, const double* b, const double* h, const double* hu, const double* hv, Inter it,
+                  const double* theta, double dt, AdjBuf a, FaceSums S, double* lb, double* lh, double* lhu,
+                  double* lhv) {
+  pdl_enter();
+  // slope derivatives: [d][q] of ga / gc, on the tile plus a ring (rows 0..9, cols 0..33)
+  __shared__ double sga[2][4][AT_Y + 2][AT_X + 2];
+  __shared__ double sgc[2][4][AT_Y + 2][AT_X + 2];
+  const int tx = threadIdx.x, ty = threadIdx.y, t = ty * AT_X + tx;
+  const int i0 = blockIdx.x * AT_X, j0 = blockIdx.y * AT_Y;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool valid = i < g.W && j < g.H;
+  const int k = j * g.W + i;
+  double db = 0, dh = 0, dU = 0, dV = 0, dhu = 0, dhv = 0;
+  if (valid) {
+    double ls[2][4];
+    double xb, xh, xU, xV, yb, yh, yU, yV;
+    face_sums(g, S, 0, i, j, k, xb, xh, xU, xV, ls[0]);
+    face_sums(g, S, 1, i, j, k, yb, yh, yU, yV, ls[1]);
+    db = xb + yb; dh = xh + yh; dU = xU + yU; dV = xV + yV;
     {
-      double lo = 0, lh = 0;
-      if (theta[k] < 1) theta_adj(g, it, theta, h, dt, a, k, lo, lh);
-      dh += lh;
+      double lo = 0, lhq = 0;
+      if (theta[k] < 1) theta_adj(g, it, theta, h, dt, a, k, lo, lhq);
+      dh += lhq;
     }
-    double dhu = 0, dhv = 0;
     const bool interior = i >= 2 && i < g.W - 2 && j >= 2 && j < g.H - 2;
-    if (interior && g.order >= 2) {                  // bed term, src/swe.mjs:570-598 (Cartesian)
-      const double bk = b[k], eC = bk + h[k];
-      for (int d = 0; d < 2; d++) {
-        const double sE = it.s[4 * d][k], sB = it.s[4 * d + 1][k];
-        const double aP = eC + 0.5 * sE - (bk + 0.5 * sB), aM = eC - 0.5 * sE - (bk - 0.5 * sB);
-        const double hP = swe::jmax0(aP), hM = swe::jmax0(aM);
-        const double div = d == 0 ? g.dxRow[j] : g.bedPhi[j];
-        const double lterm = a.lR[1 + d][k];
-        const double lhPM = lterm * (-SWE_G * 0.5 * sB / div);
-        const double ldb = lterm * (-SWE_G * 0.5 * (hP + hM)) / div;
-        double leC = 0;
-        if (aP > 0) { leC += lhPM; ls[4 * d] += 0.5 * lhPM; db -= lhPM; ls[4 * d + 1] -= 0.5 * lhPM; }
-        if (aM > 0) { leC += lhPM; ls[4 * d] -= 0.5 * lhPM; db -= lhPM; ls[4 * d + 1] += 0.5 * lhPM; }
-        ls[4 * d + 1] += ldb;
-        db += leC; dh += leC;
-      }
+    if (interior && g.order >= 2) {
+      bed_term_adj(g, b, h, it, a, 0, j, k, ls[0], db, dh);
+      bed_term_adj(g, b, h, it, a, 1, j, k, ls[1], db, dh);
     }
     if (interior && g.coriolis != 0 && g.coriolis == g.coriolis) {   // rhu += f hv; rhv -= f hu
       dhv += g.coriolis * a.lR[1][k];
       dhu -= g.coriolis * a.lR[2][k];
     }
-    a.dir[0][k] = db; a.dir[1][k] = dh; a.dir[2][k] = dU; a.dir[3][k] = dV;
-    lhu[k] += dhu; lhv[k] += dhv;
-    // slopes: s = lim(X[k] - X[km], X[kp] - X[k]) for X = eta, b, U, V
+#pragma unroll
     for (int d = 0; d < 2; d++) {
-      double ga[4] = {0, 0, 0, 0}, gc[4] = {0, 0, 0, 0};
-      if (g.order >= 2 && i >= 1 && i < g.W - 1 && j >= 1 && j < g.H - 1) {
-        const int kp = d == 0 ? k + 1 : k + g.W, km = d == 0 ? k - 1 : k - g.W;
-        if (!(h[k] <= g.minDepth || h[kp] <= g.minDepth || h[km] <= g.minDepth)) {
-          const double eC = b[k] + h[k], eP = b[kp] + h[kp], eM = b[km] + h[km];
-          const double X0[4] = {eC - eM, b[k] - b[km], it.U[k] - it.U[km], it.V[k] - it.V[km]};
-          const double X1[4] = {eP - eC, b[kp] - b[k], it.U[kp] - it.U[k], it.V[kp] - it.V[k]};
-          for (int q = 0; q < 4; q++) {
-            double da, dc;
-            swe::adj::limiter_grad(g.lim, X0[q], X1[q], da, dc);
-            ga[q] = ls[4 * d + q] * da;
-            gc[q] = ls[4 * d + q] * dc;
-          }
-        }
-      }
-      for (int q = 0; q < 4; q++) { a.gs[8 * d + 2 * q][k] = ga[q]; a.gs[8 * d + 2 * q + 1][k] = gc[q]; }
+      double ga[4], gc[4];
+      limiter_adj(g, b, h, it, d, i, j, k, ls[d], ga, gc);
+#pragma unroll
+      for (int q = 0; q < 4; q++) { sga[d][q][ty + 1][tx + 1] = ga[q]; sgc[d][q][ty + 1][tx + 1] = gc[q]; }
     }
   }
-}
-
-// Per cell: the slopes' derivatives land on the cell and its neighbours;
-// eta = b + h, and the velocities' reverse.
-__global__ void k_adj_cells_final(Geo g, const double* h, const double* hu, const double* hv, Inter it, AdjBuf a,
-                                  double* lb, double* lh, double* lhu, double* lhv) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < g.W * g.H; k += gridDim.x * blockDim.x) {
-    const int i = k % g.W, j = k / g.W;
-    double lX[4] = {0, 0, 0, 0};                     // eta, b, U, V
-    for (int d = 0; d < 2; d++) {
-      const int st = d == 0 ? 1 : g.W;
-      const bool hasM = d == 0 ? i >= 1 : j >= 1;
-      const bool hasP = d == 0 ? i + 1 < g.W : j + 1 < g.H;
+  // The ring: what a neighbour outside the tile sends in.  Left column: its
+  // x-slope gc; right column: its x-slope ga; bottom row: its y-slope gc;
+  // top row: its y-slope ga.  Threads 0..79 take one ring cell each.
+  if (t < 2 * AT_Y + 2 * AT_X) {
+    int ri, rj, d, sx, sy;
+    bool want_c;
+    if (t < AT_Y) { ri = i0 - 1; rj = j0 + t; d = 0; want_c = true; sx = 0; sy = t + 1; }
+    else if (t < 2 * AT_Y) { ri = i0 + AT_X; rj = j0 + t - AT_Y; d = 0; want_c = false; sx = AT_X + 1; sy = t - AT_Y + 1; }
+    else if (t < 2 * AT_Y + AT_X) { ri = i0 + t - 2 * AT_Y; rj = j0 - 1; d = 1; want_c = true; sx = ri - i0 + 1; sy = 0; }
+    else { ri = i0 + t - 2 * AT_Y - AT_X; rj = j0 + AT_Y; d = 1; want_c = false; sx = ri - i0 + 1; sy = AT_Y + 1; }
+    if (ri >= 0 && ri < g.W && rj >= 0 && rj < g.H) {
+      const int rk = rj * g.W + ri;
+      double ls[4], rb, rh, rU, rV;
+      dir_slopes(g, b, h, it, a, S, d, ri, rj, rk, ls, rb, rh, rU, rV);
+      double ga[4], gc[4];
+      limiter_adj(g, b, h, it, d, ri, rj, rk, ls, ga, gc);
+#pragma unroll
       for (int q = 0; q < 4; q++) {
-        const double* GA = a.gs[8 * d + 2 * q];
-        const double* GC = a.gs[8 * d + 2 * q + 1];
-        double v = GA[k] - GC[k];                    // own slope: a = X[k] - X[km], c = X[kp] - X[k]
-        if (hasM) v += GC[k - st];                   // slope of km: its c = X[k] - X[km]
-        if (hasP) v -= GA[k + st];                   // slope of kp: its a = X[kp] - X[k]
-        lX[q] += v;
+        if (want_c) sgc[d][q][sy][sx] = gc[q]; else sga[d][q][sy][sx] = ga[q];
       }
     }
-    const double lU = lX[2] + a.dir[2][k], lV = lX[3] + a.dir[3][k];
-    double dqU, dhU, dqV, dhV;
-    swe::adj::vel_grad(hu[k], h[k], g.eps4, dqU, dhU);
-    swe::adj::vel_grad(hv[k], h[k], g.eps4, dqV, dhV);
-    lb[k] += lX[0] + lX[1] + a.dir[0][k];
-    lh[k] += lX[0] + a.dir[1][k] + lU * dhU + lV * dhV;
-    lhu[k] += lU * dqU;
-    lhv[k] += lV * dqV;
   }
+  __syncthreads();
+  if (!valid) return;
+  double lX[4] = {0, 0, 0, 0};                       // eta, b, U, V
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+    const bool hasM = d == 0 ? i >= 1 : j >= 1;
+    const bool hasP = d == 0 ? i + 1 < g.W : j + 1 < g.H;
+    const int mx = d == 0 ? tx : tx + 1, my = d == 0 ? ty + 1 : ty;
+    const int px = d == 0 ? tx + 2 : tx + 1, py = d == 0 ? ty + 1 : ty + 2;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      double v = sga[d][q][ty + 1][tx + 1] - sgc[d][q][ty + 1][tx + 1];
+      if (hasM) v += sgc[d][q][my][mx];
+      if (hasP) v -= sga[d][q][py][px];
+      lX[q] += v;
+    }
+  }
+  const double lU = lX[2] + dU, lV = lX[3] + dV;
+  double dqU, dhU, dqV, dhV;
+  swe::adj::vel_grad(hu[k], h[k], g.eps4, dqU, dhU);
+  swe::adj::vel_grad(hv[k], h[k], g.eps4, dqV, dhV);
+  lb[k] += lX[0] + lX[1] + db;
+  lh[k] += lX[0] + dh + lU * dhU + lV * dhV;
+  lhu[k] = (lhu[k] + dhu) + lU * dqU;
+  lhv[k] = (lhv[k] + dhv) + lV * dqV;
 }
 
 // ---- the rest of the step backwards ----------------------------------------
@@ -345,6 +459,7 @@ __device__ __forceinline__ void adj_bc_move(int W, int gi, int gj, int sk, doubl
 }
 
 __global__ void k_adj_bc(int nx, int ny, double* lb, double* lh, double* lhu, double* lhv) {
+  pdl_enter();
   const int W = nx + 4;
   const int rows[4] = {0, 1, ny - 2, ny - 1};
   const int cols[4] = {0, 1, nx - 2, nx - 1};
@@ -397,51 +512,77 @@ __global__ void k_adj_bc(int nx, int ny, double* lb, double* lh, double* lhu, do
   }
 }
 
-// dryClean (src/swe.mjs:734-745) backwards, from the pre-clean depth:
-// a floored depth and zeroed momenta pass no adjoint.  Ghost outputs are
-// dead (the next ghost fill overwrites them), so their adjoints are cleared.
-__global__ void k_adj_dryclean(int W, int H, double minDepth, const double* hpre, double* lh, double* lhu, double* lhv) {
+// The end of the step backwards, one pass per cell: friction (as
+// k_adj_friction), dryClean from the stage-2 pre-clean depth (as
+// k_adj_dryclean), then A = 0.5 (W1 + B + dt R2), which sends
+// lB = 0.5 lA, lR = 0.5 dt lA and leaves lA <- 0.5 lA (= lW1).
+__device__ __forceinline__ void friction_rev(double minDepth, double eps4, double n, double dt, double hk,
+                                             double qu, double qv, double& a0, double& a1, double& a2,
+                                             double* ln, int k) {
+  if (!(n != 0 && n == n)) return;                  // identity (scalar n == 0 skips entirely)
+  if (hk <= minDepth) { a1 = 0; a2 = 0; return; }
+  const double den = swe::vel_den(hk, eps4);
+  const double u = swe::vel_num(qu, hk) / den, v = swe::vel_num(qv, hk) / den;
+  const double speed = hypot(u, v);
+  if (speed < 1e-14) return;
+  const double P = pow(hk, 4.0 / 3.0);
+  const double K = dt * SWE_G * n * n;
+  const double denom = 1 + K * speed / P;
+  const double ghu = a1, ghv = a2;
+  const double lden = -(ghu * qu + ghv * qv) / (denom * denom);
+  double gh = 0, gq = ghu / denom, gr = ghv / denom;
+  const double lspeed = lden * K / P;
+  const double lP = -lden * K * speed / (P * P);
+  if (ln) ln[k] += lden * dt * SWE_G * 2 * n * speed / P;
+  gh += lP * (4.0 / 3.0) * P / hk;
+  const double lu = lspeed * u / speed, lv = lspeed * v / speed;
+  double dqU, dhU, dqV, dhV;
+  swe::adj::vel_grad(qu, hk, eps4, dqU, dhU);
+  swe::adj::vel_grad(qv, hk, eps4, dqV, dhV);
+  gq += lu * dqU; gr += lv * dqV; gh += lu * dhU + lv * dhV;
+  a0 += gh; a1 = gq; a2 = gr;
+}
+
+__global__ void k_adj_tail2(int W, int H, double minDepth, double eps4, double manning, const double* nfield,
+                            double dt, const double* fh, const double* fhu, const double* fhv, const double* hA,
+                            double* lA0, double* lA1, double* lA2, double* ln, double* lB0, double* lB1,
+                            double* lB2, double* lR0, double* lR1, double* lR2) {
+  pdl_enter();
+  const double hdt = 0.5 * dt;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < W * H; k += gridDim.x * blockDim.x) {
     const int i = k % W, j = k / W;
-    if (!(i >= 2 && i < W - 2 && j >= 2 && j < H - 2)) continue;
-    const double hp = hpre[k];
-    const double hc = hp < 0 ? 0 : hp;
-    if (hp < 0) lh[k] = 0;
-    if (hc <= minDepth) { lhu[k] = 0; lhv[k] = 0; }
+    double a0 = lA0[k], a1 = lA1[k], a2 = lA2[k];
+    if (i >= 2 && i < W - 2 && j >= 2 && j < H - 2) {
+      friction_rev(minDepth, eps4, nfield ? nfield[k] : manning, dt, fh[k], fhu[k], fhv[k], a0, a1, a2, ln, k);
+      const double hp = hA[k];
+      const double hc = hp < 0 ? 0 : hp;
+      if (hp < 0) a0 = 0;
+      if (hc <= minDepth) { a1 = 0; a2 = 0; }
+    }
+    lB0[k] = 0.5 * a0; lB1[k] = 0.5 * a1; lB2[k] = 0.5 * a2;
+    lR0[k] = hdt * a0; lR1[k] = hdt * a1; lR2[k] = hdt * a2;
+    lA0[k] = 0.5 * a0; lA1[k] = 0.5 * a1; lA2[k] = 0.5 * a2;
   }
 }
 
-// applyFriction (src/swe.mjs:659-704) backwards, from the post-dryClean state.
-__global__ void k_adj_friction(int W, int H, double minDepth, double eps4, double manning, const double* nfield,
-                               double dt, const double* h, const double* hu, const double* hv,
-                               double* lh, double* lhu, double* lhv, double* ln) {
+// Stage 1 backwards after its ghost map: dryClean from the stage-1
+// pre-clean depth, then B = W1 + dt R1: lW1 += lB, lR = dt lB (lB is dead
+// afterwards, so the cleaned values are not stored).
+__global__ void k_adj_tail1(int W, int H, double minDepth, double dt, const double* hB, const double* lB0,
+                            const double* lB1, const double* lB2, double* lA0, double* lA1, double* lA2,
+                            double* lR0, double* lR1, double* lR2) {
+  pdl_enter();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < W * H; k += gridDim.x * blockDim.x) {
     const int i = k % W, j = k / W;
-    if (!(i >= 2 && i < W - 2 && j >= 2 && j < H - 2)) continue;
-    const double n = nfield ? nfield[k] : manning;
-    if (!(n != 0 && n == n)) continue;               // identity (scalar n == 0 skips entirely)
-    const double hk = h[k];
-    if (hk <= minDepth) { lhu[k] = 0; lhv[k] = 0; continue; }
-    const double den = swe::vel_den(hk, eps4);
-    const double u = swe::vel_num(hu[k], hk) / den, v = swe::vel_num(hv[k], hk) / den;
-    const double speed = hypot(u, v);
-    if (speed < 1e-14) continue;
-    const double P = pow(hk, 4.0 / 3.0);
-    const double K = dt * SWE_G * n * n;
-    const double denom = 1 + K * speed / P;
-    const double ghu = lhu[k], ghv = lhv[k];
-    const double lden = -(ghu * hu[k] + ghv * hv[k]) / (denom * denom);
-    double gh = 0, gq = ghu / denom, gr = ghv / denom;
-    const double lspeed = lden * K / P;
-    const double lP = -lden * K * speed / (P * P);
-    if (ln) ln[k] += lden * dt * SWE_G * 2 * n * speed / P;
-    gh += lP * (4.0 / 3.0) * P / hk;
-    const double lu = lspeed * u / speed, lv = lspeed * v / speed;
-    double dqU, dhU, dqV, dhV;
-    swe::adj::vel_grad(hu[k], hk, eps4, dqU, dhU);
-    swe::adj::vel_grad(hv[k], hk, eps4, dqV, dhV);
-    gq += lu * dqU; gr += lv * dqV; gh += lu * dhU + lv * dhV;
-    lh[k] += gh; lhu[k] = gq; lhv[k] = gr;
+    double b0 = lB0[k], b1 = lB1[k], b2 = lB2[k];
+    if (i >= 2 && i < W - 2 && j >= 2 && j < H - 2) {
+      const double hp = hB[k];
+      const double hc = hp < 0 ? 0 : hp;
+      if (hp < 0) b0 = 0;
+      if (hc <= minDepth) { b1 = 0; b2 = 0; }
+    }
+    lA0[k] += 1.0 * b0; lA1[k] += 1.0 * b1; lA2[k] += 1.0 * b2;
+    lR0[k] = dt * b0; lR1[k] = dt * b1; lR2[k] = dt * b2;
   }
 }
 
@@ -451,6 +592,7 @@ __global__ void k_adj_friction(int W, int H, double minDepth, double eps4, doubl
 constexpr int MISFIT_THREADS = 256;
 __global__ void k_misfit(const double* b, const double* h, const int* gk, const double* obs, int ng,
                          double* J, double* eta_out) {
+  pdl_enter();
   __shared__ double r2[MISFIT_THREADS];
   double s = 0;
   if (threadIdx.x == 0) s = *J;
@@ -473,6 +615,7 @@ __global__ void k_misfit(const double* b, const double* h, const int* gk, const 
 // sums are those of a sequential pass over the gauges; groups run in parallel.
 __global__ void k_adj_misfit(const double* b, const double* h, const int* gcell, const int* goff, const int* gidx,
                              int ngroups, const double* obs, double* lb, double* lh) {
+  pdl_enter();
   for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < ngroups; u += gridDim.x * blockDim.x) {
     const int k = gcell[u];
     const double e = b[k] + h[k];
@@ -487,10 +630,22 @@ __global__ void k_adj_misfit(const double* b, const double* h, const int* gcell,
   }
 }
 __global__ void k_set_dt(Control* ctl, const double* dts, int s) {
+  pdl_enter();
   if (threadIdx.x == 0) { ctl->dt = dts[s]; ctl->stop = 0; }
 }
 __global__ void k_record_dt(const Control* ctl, double* dts, int s) {
+  pdl_enter();
   if (threadIdx.x == 0) dts[s] = ctl->dt;
+}
+// dst[q] = src[q] for q < nf (checkpoints and the segment tape's copies of
+// the state, as a kernel so that the stepping chain stays one of kernels).
+__global__ void k_copy(size_t n, int nf, double* d0, double* d1, double* d2, const double* s0, const double* s1,
+                       const double* s2) {
+  pdl_enter();
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    d0[k] = s0[k];
+    if (nf > 1) { d1[k] = s1[k]; d2[k] = s2[k]; }
+  }
 }
 // h0 = max(0, eta0 - b): d h0 / d b = -1 where eta0 - b > 0 (interior).
 __global__ void k_adj_initial(int W, int H, const double* b, const double* eta0, const double* lh, double* lb) {
@@ -506,29 +661,6 @@ __global__ void k_init_state(int N, const double* b, const double* eta0, double*
     h[k] = swe::jmax0(eta0[k] - b[k]); hu[k] = 0; hv[k] = 0;
   }
 }
-// dryClean's result (src/swe.mjs:734-745) on the interior, copying ghosts as they are.
-// The stage combinations backwards, three fields at once.
-// A = 0.5 (W1 + B + dt R2):  lB = 0.5 lA, lR = 0.5 dt lA, lA <- 0.5 lA (= lW1).
-__global__ void k_split_stage2(int N, double dt, double* lA0, double* lA1, double* lA2, double* lB0, double* lB1,
-                               double* lB2, double* lR0, double* lR1, double* lR2) {
-  const double hdt = 0.5 * dt;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
-    const double a0 = lA0[k], a1 = lA1[k], a2 = lA2[k];
-    lB0[k] = 0.5 * a0; lB1[k] = 0.5 * a1; lB2[k] = 0.5 * a2;
-    lR0[k] = hdt * a0; lR1[k] = hdt * a1; lR2[k] = hdt * a2;
-    lA0[k] = 0.5 * a0; lA1[k] = 0.5 * a1; lA2[k] = 0.5 * a2;
-  }
-}
-// B = W1 + dt R1:  lW1 += lB, lR = dt lB.
-__global__ void k_split_stage1(int N, double dt, const double* lB0, const double* lB1, const double* lB2,
-                               double* lA0, double* lA1, double* lA2, double* lR0, double* lR1, double* lR2) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
-    const double b0 = lB0[k], b1 = lB1[k], b2 = lB2[k];
-    lA0[k] += 1.0 * b0; lA1[k] += 1.0 * b1; lA2[k] += 1.0 * b2;
-    lR0[k] = dt * b0; lR1[k] = dt * b1; lR2[k] = dt * b2;
-  }
-}
-
 }  // namespace
 
 struct swe_adjoint {
@@ -546,6 +678,7 @@ struct swe_adjoint {
   int ngroups = 0;
   double *lA[3], *lB[3], *lb, *ln;
   AdjBuf ab;
+  FaceSums fs;                     // per-cell face sums of the tiled reverse kernels
   double *part;
   Control* ctl;
   int nblocks;
@@ -554,6 +687,7 @@ struct swe_adjoint {
   dim3 sgrid;
   int pcap = 0;                    // partial slots per kind (the most tiles either kernel uses)
   bool forward_done = false;
+  bool pdl = true;                 // programmatic dependent launch between the stepping kernels
   bool fixed_dt = false;         // forward uses the given dt sequence instead of maxDt()
   std::vector<double> dts_host;  // the dt sequence, read once per backward pass
 };
@@ -604,6 +738,32 @@ int G1(const swe_adjoint* s) { return std::min(4096, (s->N + 255) / 256); }
 int bcb(const swe_adjoint* s) { return (4 * s->o.ny + 4 * (s->o.nx + 4) + 255) / 256; }
 int adjbc_blocks(const swe_adjoint* s) { return (4 * s->o.nx + 4 * s->o.ny + 255) / 256; }
 
+// A launch on the handle's stream that, with `pdl`, may be scheduled while
+// the previous kernel drains (every kernel here waits for its predecessors
+// in pdl_enter before touching memory).  The first kernel after a memset or
+// a copy is launched without it.
+template <typename... KArgs, typename... Args>
+cudaError_t launch(const swe_adjoint* s, bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s->st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = (pdl && s->pdl) ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+#define LAUNCH(...) CU(launch(s, true, __VA_ARGS__))
+
+int copy3(swe_adjoint* s, double* const* dst, double* const* src, bool pdl = true) {
+  CU(launch(s, pdl, k_copy, dim3(G1(s)), dim3(256), (size_t)s->N, 3, dst[0], dst[1], dst[2],
+            (const double*)src[0], (const double*)src[1], (const double*)src[2]));
+  return SWE_OK;
+}
+
 // One forward step of state X in place, dt from the device control block
 // (set by k_set_dt or, when auto_dt, from the CFL rate).
 int fwd_step(swe_adjoint* s, double* const* X, bool auto_dt, int step_index) {
@@ -611,29 +771,26 @@ int fwd_step(swe_adjoint* s, double* const* X, bool auto_dt, int step_index) {
     swe::PrepArgs p;
     std::memset(&p, 0, sizeof p);
     p.mode = 1; p.cfl = s->o.cfl; p.t_end = INFINITY;
-    swe::k_prepare<<<1, 32, 0, s->st>>>(s->ctl, p);
+    LAUNCH(swe::k_prepare, dim3(1), dim3(32), s->ctl, p);
   } else {
-    k_set_dt<<<1, 32, 0, s->st>>>(s->ctl, s->dts, step_index);
+    LAUNCH(k_set_dt, dim3(1), dim3(32), s->ctl, (const double*)s->dts, step_index);
   }
-  swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, X), s->ctl, 0);
+  const dim3 spb(swe::SP_THREADS);
+  const int nparts = (int)(s->sgrid.x * s->sgrid.y);
+  LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, X), (const Control*)s->ctl, 0);
   const StageArgs a1 = stage_args(s, X, s->Bf);
-  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
-  swe::k_split_cells<1><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, s->sb, s->ctl);
-  swe::k_split_close<1><<<1, swe::SP_THREADS, 0, s->st>>>(a1, s->ctl, (int)(s->sgrid.x * s->sgrid.y));
-  swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, s->Bf), s->ctl, 0);
+  LAUNCH(swe::k_split_faces, s->sgrid, spb, a1, s->sb, s->ctl);
+  LAUNCH(swe::k_split_cells<1>, s->sgrid, spb, a1, s->sb, s->ctl);
+  LAUNCH(swe::k_split_close<1>, dim3(1), spb, a1, s->ctl, nparts);
+  LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, s->Bf), (const Control*)s->ctl, 0);
   const StageArgs a2 = stage_args(s, s->Bf, X);
-  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
-  swe::k_split_cells<2><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, s->sb, s->ctl);
-  swe::k_split_close<2><<<1, swe::SP_THREADS, 0, s->st>>>(a2, s->ctl, (int)(s->sgrid.x * s->sgrid.y));
-  CU(cudaGetLastError());
-  if (auto_dt) k_record_dt<<<1, 32, 0, s->st>>>(s->ctl, s->dts, step_index);
+  LAUNCH(swe::k_split_faces, s->sgrid, spb, a2, s->sb, s->ctl);
+  LAUNCH(swe::k_split_cells<2>, s->sgrid, spb, a2, s->sb, s->ctl);
+  LAUNCH(swe::k_split_close<2>, dim3(1), spb, a2, s->ctl, nparts);
+  if (auto_dt) LAUNCH(k_record_dt, dim3(1), dim3(32), (const Control*)s->ctl, s->dts, step_index);
   return SWE_OK;
 }
 
-void copy3(swe_adjoint* s, double* const* dst, double* const* src) {
-  for (int q = 0; q < 3; q++)
-    cudaMemcpyAsync(dst[q], src[q], sizeof(double) * s->N, cudaMemcpyDeviceToDevice, s->st);
-}
 
 // R^T: given ab.lR (adjoint of rh, rhu, rhv over all cells) at state X (ghosts
 // filled), add into lX (h, hu, hv) and lb.
@@ -641,25 +798,21 @@ void copy3(swe_adjoint* s, double* const* dst, double* const* src) {
 int residual_adjoint(swe_adjoint* s, double* const* X, const Inter& it, const double* theta, double dt,
                      double* const* lX) {
   const Geo g = geo_of(s);
-  const int gb = G1(s);
-  const int fcb = std::min(148 * 4 * 4, (s->N + FACES_CORE_THREADS - 1) / FACES_CORE_THREADS);
-  if (SWE_FACES_CORE_SPLIT) {
-    k_adj_faces_core<0><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, theta, dt, s->ab);
-    k_adj_faces_core<1><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, theta, dt, s->ab);
-  } else {
-    k_adj_faces_core<2><<<fcb, FACES_CORE_THREADS, 0, s->st>>>(g, s->b, X[0], it, theta, dt, s->ab);
-  }
-  k_adj_cells<<<gb, 256, 0, s->st>>>(g, s->b, X[0], X[1], X[2], it, theta, dt, s->ab, lX[1], lX[2]);
-  k_adj_cells_final<<<gb, 256, 0, s->st>>>(g, X[0], X[1], X[2], it, s->ab, s->lb, lX[0], lX[1], lX[2]);
-  CU(cudaGetLastError());
+  const int ntx = (s->W + AT_X - 1) / AT_X;
+  const double* b = s->b;
+  const double* h = X[0];
+  LAUNCH(k_adj_xfaces, dim3(ntx, (s->H + AT_XROWS - 1) / AT_XROWS), dim3(AT_X, AT_XROWS), g, b, h, it, theta, dt,
+         s->ab, s->fs);
+  LAUNCH(k_adj_yfaces, dim3(ntx, (s->H + AT_Y - 1) / AT_Y), dim3(AT_X, AT_Y), g, b, h, it, theta, dt, s->ab, s->fs);
+  LAUNCH(k_adj_cells_tiled, dim3(ntx, (s->H + AT_Y - 1) / AT_Y), dim3(AT_X, AT_Y), g, b, h, (const double*)X[1],
+         (const double*)X[2], it, theta, dt, s->ab, s->fs, s->lb, lX[0], lX[1], lX[2]);
   return SWE_OK;
 }
 
 // One step's tape: what the reverse of the step reads.  The segment pass
-// writes it while stepping forward from the segment's checkpoint; the step
-// is the same arithmetic as the fused kernels (their updates are these
-// elementwise expressions, their residual is k_stage<0>), so the states are
-// the forward pass's own.
+// writes it while stepping forward from the segment's checkpoint with the
+// same tiled stage kernels and the recorded dt, so the states are the
+// forward pass's own.
 struct Tape {
   double* W1[3];   // stage-1 input with ghosts filled
   double* th1;     // positivity limiter of stage 1
@@ -711,27 +864,28 @@ swe::SplitBufs tape_bufs(const swe_adjoint* s, const Inter& it) {
 // kernels write the limiter, the depth before dryClean and friction's input
 // as they go.
 int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
-  const int N = s->N;
-  k_set_dt<<<1, 32, 0, s->st>>>(s->ctl, s->dts, k);
-  copy3(s, T.W1, X);
-  swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, T.W1), s->ctl, 0);
+  const dim3 spb(swe::SP_THREADS);
+  const int nparts = (int)(s->sgrid.x * s->sgrid.y);
+  LAUNCH(k_set_dt, dim3(1), dim3(32), s->ctl, (const double*)s->dts, k);
+  if (int rc = copy3(s, T.W1, X)) return rc;
+  LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, T.W1), (const Control*)s->ctl, 0);
   StageArgs a1 = stage_args(s, T.W1, T.Bp);
   a1.tape_th = T.th1; a1.tape_hpre = T.hB;
   const swe::SplitBufs b1 = tape_bufs(s, T.it1);
-  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, b1, s->ctl);
-  swe::k_split_cells<1><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a1, b1, s->ctl);
-  swe::k_split_close<1><<<1, swe::SP_THREADS, 0, s->st>>>(a1, s->ctl, (int)(s->sgrid.x * s->sgrid.y));
-  swe::k_apply_bc<<<bcb(s), 256, 0, s->st>>>(bc_args(s, T.Bp), s->ctl, 0);
-  copy3(s, X, T.W1);                               // U0 of the in-place stage 2
+  LAUNCH(swe::k_split_faces, s->sgrid, spb, a1, b1, s->ctl);
+  LAUNCH(swe::k_split_cells<1>, s->sgrid, spb, a1, b1, s->ctl);
+  LAUNCH(swe::k_split_close<1>, dim3(1), spb, a1, s->ctl, nparts);
+  LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, T.Bp), (const Control*)s->ctl, 0);
+  if (int rc = copy3(s, X, T.W1)) return rc;       // U0 of the in-place stage 2
   StageArgs a2 = stage_args(s, T.Bp, X);
   a2.tape_th = T.th2; a2.tape_hpre = T.hA;
   for (int q = 0; q < 3; q++) a2.tape_pre[q] = T.Bf[q];
   const swe::SplitBufs b2 = tape_bufs(s, T.it2);
-  swe::k_split_faces<<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, b2, s->ctl);
-  swe::k_split_cells<2><<<s->sgrid, swe::SP_THREADS, 0, s->st>>>(a2, b2, s->ctl);
-  swe::k_split_close<2><<<1, swe::SP_THREADS, 0, s->st>>>(a2, s->ctl, (int)(s->sgrid.x * s->sgrid.y));
-  cudaMemcpyAsync(T.hX, X[0], sizeof(double) * N, cudaMemcpyDeviceToDevice, s->st);
-  CU(cudaGetLastError());
+  LAUNCH(swe::k_split_faces, s->sgrid, spb, a2, b2, s->ctl);
+  LAUNCH(swe::k_split_cells<2>, s->sgrid, spb, a2, b2, s->ctl);
+  LAUNCH(swe::k_split_close<2>, dim3(1), spb, a2, s->ctl, nparts);
+  LAUNCH(k_copy, dim3(G1(s)), dim3(256), (size_t)s->N, 1, T.hX, (double*)nullptr, (double*)nullptr,
+         (const double*)X[0], (const double*)nullptr, (const double*)nullptr);
   return SWE_OK;
 }
 
@@ -739,26 +893,25 @@ int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
 // (interior), on exit the adjoint of its input (interior); lb and ln
 // accumulate.
 int reverse_step(swe_adjoint* s, int k, const Tape& T) {
-  const int N = s->N, gb = G1(s);
+  const int gb = G1(s);
   const double dt = s->dts_host[k];
   double* lA[3] = {s->lA[0], s->lA[1], s->lA[2]};
   double* lB[3] = {s->lB[0], s->lB[1], s->lB[2]};
-  k_adj_friction<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, s->eps4, s->o.manning, s->nfield, dt,
-                                        T.Bf[0], T.Bf[1], T.Bf[2], lA[0], lA[1], lA[2], s->ln);
-  k_adj_dryclean<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, T.hA, lA[0], lA[1], lA[2]);
-  // A = 0.5 (W1 + Bp + dt R2): lB = 0.5 lA, lR2 = 0.5 dt lA, lW1 = 0.5 lA
-  k_split_stage2<<<gb, 256, 0, s->st>>>(N, dt, lA[0], lA[1], lA[2], lB[0], lB[1], lB[2], s->ab.lR[0],
-                                        s->ab.lR[1], s->ab.lR[2]);
+  // friction, dryClean, A = 0.5 (W1 + Bp + dt R2) backwards in one pass
+  LAUNCH(k_adj_tail2, dim3(gb), dim3(256), s->W, s->H, s->o.min_depth, s->eps4, s->o.manning,
+         (const double*)s->nfield, dt, (const double*)T.Bf[0], (const double*)T.Bf[1], (const double*)T.Bf[2],
+         (const double*)T.hA, lA[0], lA[1], lA[2], s->ln, lB[0], lB[1], lB[2], s->ab.lR[0], s->ab.lR[1],
+         s->ab.lR[2]);
   int rc = residual_adjoint(s, T.Bp, T.it2, T.th2, dt, lB);
   if (rc) return rc;
-  k_adj_bc<<<adjbc_blocks(s), 256, 0, s->st>>>(s->o.nx, s->o.ny, s->lb, lB[0], lB[1], lB[2]);
-  k_adj_dryclean<<<gb, 256, 0, s->st>>>(s->W, s->H, s->o.min_depth, T.hB, lB[0], lB[1], lB[2]);
-  // B = W1 + dt R1 (all cells): lW1 += lB, lR1 = dt lB
-  k_split_stage1<<<gb, 256, 0, s->st>>>(N, dt, lB[0], lB[1], lB[2], lA[0], lA[1], lA[2], s->ab.lR[0],
-                                        s->ab.lR[1], s->ab.lR[2]);
+  LAUNCH(k_adj_bc, dim3(adjbc_blocks(s)), dim3(256), s->o.nx, s->o.ny, s->lb, lB[0], lB[1], lB[2]);
+  // dryClean and B = W1 + dt R1 backwards: lW1 += lB, lR1 = dt lB
+  LAUNCH(k_adj_tail1, dim3(gb), dim3(256), s->W, s->H, s->o.min_depth, dt, (const double*)T.hB,
+         (const double*)lB[0], (const double*)lB[1], (const double*)lB[2], lA[0], lA[1], lA[2], s->ab.lR[0],
+         s->ab.lR[1], s->ab.lR[2]);
   rc = residual_adjoint(s, T.W1, T.it1, T.th1, dt, lA);
   if (rc) return rc;
-  k_adj_bc<<<adjbc_blocks(s), 256, 0, s->st>>>(s->o.nx, s->o.ny, s->lb, lA[0], lA[1], lA[2]);
+  LAUNCH(k_adj_bc, dim3(adjbc_blocks(s)), dim3(256), s->o.nx, s->o.ny, s->lb, lA[0], lA[1], lA[2]);
   CU(cudaGetLastError());
   return SWE_OK;
 }
@@ -819,8 +972,14 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
   s->J = A(1);
   s->lb = A(N); s->ln = A(N);
   for (int q = 0; q < 3; q++) s->ab.lR[q] = A(N);
-  for (int q = 0; q < 16; q++) { s->ab.gx[q] = A(N); s->ab.gy[q] = A(N); s->ab.gs[q] = A(N); }
-  for (int q = 0; q < 4; q++) s->ab.dir[q] = A(N);
+  {
+    const int ntx = (s->W + AT_X - 1) / AT_X, nty = (s->H + AT_Y - 1) / AT_Y;
+    s->fs.ntx = ntx;
+    for (int q = 0; q < 8; q++) {
+      s->fs.sx[q] = A(N); s->fs.sy[q] = A(N);
+      s->fs.ex[q] = A((size_t)ntx * s->H); s->fs.ey[q] = A((size_t)nty * s->W);
+    }
+  }
   const int gx = (s->W + swe::SX - 1) / swe::SX, gy = (s->H + 31) / 32;
   s->grid = dim3(gx, gy);
   s->nblocks = gx * gy;
@@ -834,9 +993,13 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
   if (!ok || cudaMalloc(&s->ctl, sizeof(Control)) != cudaSuccess || cudaMalloc(&s->gk, sizeof(int) * n_gauges) != cudaSuccess)
     return bail(fail(SWE_ECUDA, "swe_adjoint_create: device allocation failed"));
   cudaMemsetAsync(s->ctl, 0, sizeof(Control), s->st);
-  cudaFuncSetAttribute(swe::k_stage<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, swe::STAGE_SMEM_BYTES);
-  cudaFuncSetAttribute(swe::k_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, swe::STAGE_SMEM_BYTES);
-  cudaFuncSetAttribute(swe::k_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, swe::STAGE_SMEM_BYTES);
+  {
+    const char* pe = std::getenv("SWE_B200_PDL");
+    s->pdl = !(pe && std::strcmp(pe, "0") == 0);
+  }
+  // room in shared memory for as many cell-kernel blocks as its registers allow
+  cudaFuncSetAttribute(k_adj_cells_tiled, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
   std::vector<double> geom((size_t)(SWE_GEOM_NROWS + 3) * s->H), sc(6);
   int rc = swe_compute_geometry(o, geom.data(), sc.data());
   if (rc) return bail(rc);
@@ -912,12 +1075,13 @@ int swe_adjoint_forward(swe_adjoint* s, double* J, double* gauge_eta) {
     if (k % s->every == 0) {
       double* dst[3] = {s->ckpt + (size_t)(k / s->every) * 3 * s->N, s->ckpt + ((size_t)(k / s->every) * 3 + 1) * s->N,
                         s->ckpt + ((size_t)(k / s->every) * 3 + 2) * s->N};
-      copy3(s, dst, s->A);
+      if (int rc = copy3(s, dst, s->A)) return rc;
     }
     int rc = fwd_step(s, s->A, !s->fixed_dt, k);
     if (rc) return rc;
-    k_misfit<<<1, MISFIT_THREADS, 0, s->st>>>(s->b, s->A[0], s->gk, s->obs + (size_t)k * s->ng, s->ng, s->J,
-                                  s->eta_series + (size_t)k * s->ng);
+    LAUNCH(k_misfit, dim3(1), dim3(MISFIT_THREADS), (const double*)s->b, (const double*)s->A[0],
+           (const int*)s->gk, (const double*)(s->obs + (size_t)k * s->ng), s->ng, s->J,
+           s->eta_series + (size_t)k * s->ng);
   }
   CU(cudaGetLastError());
   if (J) CU(cudaMemcpyAsync(J, s->J, sizeof(double), cudaMemcpyDeviceToHost, s->st));
@@ -954,16 +1118,17 @@ int swe_adjoint_backward(swe_adjoint* s, double* grad_b, double* grad_n) {
     const int k0 = sg * s->every, k1 = std::min(s->steps, k0 + s->every);
     // the segment forward from its checkpoint, recording each step's tape
     double* src[3] = {s->ckpt + (size_t)sg * 3 * N, s->ckpt + ((size_t)sg * 3 + 1) * N, s->ckpt + ((size_t)sg * 3 + 2) * N};
-    copy3(s, s->X, src);
+    // the first kernel after the memsets and the tape allocation waits for them in stream order
+    if (int rc = copy3(s, s->X, src, sg != s->nseg - 1)) return rc;
     for (int k = k0; k < k1; k++) {
       int rc = tape_step(s, s->X, k, tape_at(s, k - k0));
       if (rc) return rc;
     }
     for (int k = k1 - 1; k >= k0; k--) {
       const Tape T = tape_at(s, k - k0);
-      k_adj_misfit<<<(s->ngroups + 127) / 128, 128, 0, s->st>>>(
-          s->b, T.hX, s->gmeta, s->gmeta + s->ngroups, s->gmeta + 2 * s->ngroups + 1, s->ngroups,
-          s->obs + (size_t)k * s->ng, s->lb, s->lA[0]);
+      LAUNCH(k_adj_misfit, dim3((s->ngroups + 127) / 128), dim3(128), (const double*)s->b, (const double*)T.hX,
+             (const int*)s->gmeta, (const int*)(s->gmeta + s->ngroups), (const int*)(s->gmeta + 2 * s->ngroups + 1),
+             s->ngroups, (const double*)(s->obs + (size_t)k * s->ng), s->lb, s->lA[0]);
       int rc = reverse_step(s, k, T);
       if (rc) return rc;
     }

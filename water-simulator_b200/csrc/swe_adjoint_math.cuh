@@ -134,22 +134,23 @@ __device__ __forceinline__ void hllc_rev(double hL, double huL, double hvL, doub
     guR += gsR;
     gcR += gsR * qR;
     const double gqR = gsR * cR;
+    // q = sqrt(X), X = Y / Z: dX = dq / (2 q), dY = dX / Z, dZ = -dY X.
+    // The derivatives need no branch decision, so they take one division
+    // where the chain rule as written takes three.
     double ghStar = 0;
     if (hStar > hL && gqL != 0) {
       const double Y = 0.5 * (hStar + hL) * hStar, Z = hL * hL, X = Y / Z;
-      const double gX = gqL / (2 * qL);
-      const double gY = gX / Z, gZ = -gX * X / Z;
+      const double gY = gqL / (2 * qL * Z), gZ = -gY * X;
       ghStar += gY * (hStar + 0.5 * hL);
       ghL += gY * 0.5 * hStar + gZ * 2 * hL;
     }
     if (hStar > hR && gqR != 0) {
       const double Y = 0.5 * (hStar + hR) * hStar, Z = hR * hR, X = Y / Z;
-      const double gX = gqR / (2 * qR);
-      const double gY = gX / Z, gZ = -gX * X / Z;
+      const double gY = gqR / (2 * qR * Z), gZ = -gY * X;
       ghStar += gY * (hStar + 0.5 * hR);
       ghR += gY * 0.5 * hStar + gZ * 2 * hR;
     }
-    const double ga = ghStar * 2 * a / SWE_G;
+    const double ga = ghStar * 2 * a * (1.0 / SWE_G);
     gcL += 0.5 * ga;
     gcR += 0.5 * ga;
     guL += 0.25 * ga;
@@ -157,8 +158,9 @@ __device__ __forceinline__ void hllc_rev(double hL, double huL, double hvL, doub
   }
   if (gcL != 0 && hL > 0) ghL += gcL * SWE_G / (2 * cL);
   if (gcR != 0 && hR > 0) ghR += gcR * SWE_G / (2 * cR);
-  if (wetL) { ghuL += guL / hL; ghvL += gvL / hL; ghL -= (guL * uL + gvL * vL) / hL; }
-  if (wetR) { ghuR += guR / hR; ghvR += gvR / hR; ghR -= (guR * uR + gvR * vR) / hR; }
+  // u = hu / h backwards, one reciprocal per side
+  if (wetL) { const double r = 1 / hL; ghuL += guL * r; ghvL += gvL * r; ghL -= (guL * uL + gvL * vL) * r; }
+  if (wetR) { const double r = 1 / hR; ghuR += guR * r; ghvR += gvR * r; ghR -= (guR * uR + gvR * vR) * r; }
 }
 
 // Inputs of one face (swe_math.cuh face_flux) and their adjoints.
