@@ -183,10 +183,11 @@ constexpr int AT_Y = 8;            // rows per y-face / cell tile (256 threads)
 #ifndef SWE_ADJ_FACE_WARPS
 #define SWE_ADJ_FACE_WARPS 32
 #endif
-// The cell kernel waits on memory: four blocks per SM (64 registers,
-// 32 warps) instead of the three its natural 80 registers leave.
+// The cell kernel waits on memory, but it keeps its natural 80 registers
+// (three blocks, 24 warps per SM): capped at 64 (four blocks) or 48 (five)
+// it spills and measured slower.
 #ifndef SWE_ADJ_CELL_BLOCKS
-#define SWE_ADJ_CELL_BLOCKS 4
+#define SWE_ADJ_CELL_BLOCKS 3
 #endif
 
 struct FaceSums {
@@ -867,8 +868,9 @@ int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
   const dim3 spb(swe::SP_THREADS);
   const int nparts = (int)(s->sgrid.x * s->sgrid.y);
   LAUNCH(k_set_dt, dim3(1), dim3(32), s->ctl, (const double*)s->dts, k);
+  // the step input with its ghosts, in X (U0 of the in-place stage 2) and on the tape
+  LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, X), (const Control*)s->ctl, 0);
   if (int rc = copy3(s, T.W1, X)) return rc;
-  LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, T.W1), (const Control*)s->ctl, 0);
   StageArgs a1 = stage_args(s, T.W1, T.Bp);
   a1.tape_th = T.th1; a1.tape_hpre = T.hB;
   const swe::SplitBufs b1 = tape_bufs(s, T.it1);
@@ -876,7 +878,6 @@ int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
   LAUNCH(swe::k_split_cells<1>, s->sgrid, spb, a1, b1, s->ctl);
   LAUNCH(swe::k_split_close<1>, dim3(1), spb, a1, s->ctl, nparts);
   LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, T.Bp), (const Control*)s->ctl, 0);
-  if (int rc = copy3(s, X, T.W1)) return rc;       // U0 of the in-place stage 2
   StageArgs a2 = stage_args(s, T.Bp, X);
   a2.tape_th = T.th2; a2.tape_hpre = T.hA;
   for (int q = 0; q < 3; q++) a2.tape_pre[q] = T.Bf[q];
@@ -997,9 +998,6 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
     const char* pe = std::getenv("SWE_B200_PDL");
     s->pdl = !(pe && std::strcmp(pe, "0") == 0);
   }
-  // room in shared memory for as many cell-kernel blocks as its registers allow
-  cudaFuncSetAttribute(k_adj_cells_tiled, cudaFuncAttributePreferredSharedMemoryCarveout,
-                       (int)cudaSharedmemCarveoutMaxShared);
   std::vector<double> geom((size_t)(SWE_GEOM_NROWS + 3) * s->H), sc(6);
   int rc = swe_compute_geometry(o, geom.data(), sc.data());
   if (rc) return bail(rc);

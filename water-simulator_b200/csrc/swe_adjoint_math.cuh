@@ -58,8 +58,12 @@ __device__ __forceinline__ void hllc_rev(double hL, double huL, double hvL, doub
                                          double& ghR, double& ghuR, double& ghvR) {
   const bool wetL = hL > dry, wetR = hR > dry;
   if (!wetL && !wetR) return;
-  const double uL = wetL ? huL / hL : 0, vL = wetL ? hvL / hL : 0;
-  const double uR = wetR ? huR / hR : 0, vR = wetR ? hvR / hR : 0;
+  // u decides the wave speeds and so every branch below: the forward's own
+  // division.  v only scales the transverse flux, so a reciprocal (reused
+  // by the reverse of u = hu / h at the end) serves.
+  const double rL = wetL ? 1 / hL : 0, rR = wetR ? 1 / hR : 0;
+  const double uL = wetL ? huL / hL : 0, vL = wetL ? hvL * rL : 0;
+  const double uR = wetR ? huR / hR : 0, vR = wetR ? hvR * rR : 0;
   const double cL = sqrt(SWE_G * jmax(hL, 0)), cR = sqrt(SWE_G * jmax(hR, 0));
   double sL, sR, a = 0, hStar = 0, qL = 1, qR = 1;
   int speeds;                                       // 0 dry|wet, 1 wet|dry, 2 wet|wet
@@ -134,18 +138,18 @@ __device__ __forceinline__ void hllc_rev(double hL, double huL, double hvL, doub
     guR += gsR;
     gcR += gsR * qR;
     const double gqR = gsR * cR;
-    // q = sqrt(X), X = Y / Z: dX = dq / (2 q), dY = dX / Z, dZ = -dY X.
-    // The derivatives need no branch decision, so they take one division
-    // where the chain rule as written takes three.
+    // q = sqrt(X), X = Y / Z: dX = dq / (2 q), dY = dX / Z, dZ = -dY X with
+    // X = q^2.  The derivatives need no branch decision, so they take one
+    // division where the chain rule as written takes three.
     double ghStar = 0;
     if (hStar > hL && gqL != 0) {
-      const double Y = 0.5 * (hStar + hL) * hStar, Z = hL * hL, X = Y / Z;
+      const double Z = hL * hL, X = qL * qL;
       const double gY = gqL / (2 * qL * Z), gZ = -gY * X;
       ghStar += gY * (hStar + 0.5 * hL);
       ghL += gY * 0.5 * hStar + gZ * 2 * hL;
     }
     if (hStar > hR && gqR != 0) {
-      const double Y = 0.5 * (hStar + hR) * hStar, Z = hR * hR, X = Y / Z;
+      const double Z = hR * hR, X = qR * qR;
       const double gY = gqR / (2 * qR * Z), gZ = -gY * X;
       ghStar += gY * (hStar + 0.5 * hR);
       ghR += gY * 0.5 * hStar + gZ * 2 * hR;
@@ -156,11 +160,14 @@ __device__ __forceinline__ void hllc_rev(double hL, double huL, double hvL, doub
     guL += 0.25 * ga;
     guR -= 0.25 * ga;
   }
-  if (gcL != 0 && hL > 0) ghL += gcL * SWE_G / (2 * cL);
-  if (gcR != 0 && hR > 0) ghR += gcR * SWE_G / (2 * cR);
+  // c = sqrt(G h): dc/dh = G / (2c) = c / (2h).  c is only differentiated on
+  // a wet side (the branches above give a dry side's c no adjoint), where
+  // 1 / h is at hand.
+  if (gcL != 0 && hL > 0) ghL += gcL * 0.5 * cL * rL;
+  if (gcR != 0 && hR > 0) ghR += gcR * 0.5 * cR * rR;
   // u = hu / h backwards, one reciprocal per side
-  if (wetL) { const double r = 1 / hL; ghuL += guL * r; ghvL += gvL * r; ghL -= (guL * uL + gvL * vL) * r; }
-  if (wetR) { const double r = 1 / hR; ghuR += guR * r; ghvR += gvR * r; ghR -= (guR * uR + gvR * vR) * r; }
+  if (wetL) { ghuL += guL * rL; ghvL += gvL * rL; ghL -= (guL * uL + gvL * vL) * rL; }
+  if (wetR) { ghuR += guR * rR; ghvR += gvR * rR; ghR -= (guR * uR + gvR * vR) * rR; }
 }
 
 // Inputs of one face (swe_math.cuh face_flux) and their adjoints.
