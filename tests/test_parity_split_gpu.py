@@ -20,19 +20,24 @@ def test_the_handles_run_the_tiled_kernels(swe):
     sim.close()
 
 
-@pytest.mark.parametrize("case", ["beach", "sphere"])
+@pytest.mark.parametrize("case", ["beach", "sphere", "beach_sponge"])
 def test_tiled_and_fused_give_the_same_bits(swe, case, monkeypatch):
-    """Down to the sign of zero: the tiled pair (with its dry-tile skip)
-    against the fused kernel, after many steps of a flooding beach and of a
-    sphere with land."""
+    """Down to the sign of zero: the tiled pair (with its dry-tile skip and
+    the tiles it settles to +0 without computing them) against the fused
+    kernel, after many steps of a flooding beach, of a sphere with land, and
+    of the beach with a sponge over its dry east end (the sponge pours water
+    onto dry tiles, so no tile may settle under it)."""
     import numpy as np
     from water_simulator_b200 import workloads
 
     def make():
-        if case == "beach":
+        if case in ("beach", "beach_sponge"):
             b, h = workloads.beach_dam_break(nx=256, ny=96, dx=8.0)
             sim = swe.ShallowWater(nx=256, ny=96, dx=8.0, bed=b, eta0=b + h, manning=0.03)
             sim.boundaries = {"west": swe.flather(lambda t: 0.0, lambda t: 0.0)}
+            if case == "beach_sponge":
+                eta_ref = float(np.max(b)) + 0.5
+                sim.forcing = swe.makeSponge(sim, side="east", width=40, strength=0.05, etaRef=eta_ref)
             return sim
         c = workloads.globe_tide(nx=180, ny=90, lat0=-80.0, lat1=80.0, modes=12)
         return swe.ShallowWater(nx=180, ny=90, bed=c["b"], eta0=c["eta0"] + (c["b"] < 0) * 0.5,

@@ -56,11 +56,13 @@ struct Control {
   int stop;             // 1: the prepared step was refused (dt not > 0 or not finite)
   int status;           // sticky status bits (1: non-finite CFL rate seen)
   unsigned int counter; // last-CTA ticket
-  int pad;
+  int settled;          // tiles the tiled cell kernels settled in the last step, one in 16 counted
   // Flather tide tables (src/tide.mjs:103-107), per side
   int tide_n[4];
   double tide_msl[4], tide_ucoef[4];
   double tide_amp[4][MAX_TIDE], tide_omega[4][MAX_TIDE], tide_phase[4][MAX_TIDE];
+  int settled_next;     // the same count for the step in flight (k_prepare moves it to `settled`)
+  int pad;
 };
 
 struct Metric {   // per-row divisors (src/geometry.mjs)
@@ -124,6 +126,8 @@ __device__ __forceinline__ void prepare_one(Control* ctl, const PrepArgs& a) {
   }
   ctl->dt = dt;
   ctl->stop = (!(dt > 0) || !isfinite(dt)) ? 1 : 0;
+  ctl->settled = ctl->settled_next;
+  ctl->settled_next = 0;
   const double t = ctl->t;
   for (int s = 0; s < 4; s++) {
     if (a.fl_kind[s] == 1) {

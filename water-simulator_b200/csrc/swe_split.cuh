@@ -67,9 +67,10 @@ struct SplitBufs {
   int ntx, nty;                    // tiles per row and column of the grid
   // optional, per tile of the stage's input / output state: 1 when every
   // cell of the tile has h exactly 0 and none is a ghost cell (so nothing
-  // but a stage or the host writes it).  The cell kernel writes odry_out
-  // with the state; the face kernel reads odry_in.  Whoever else writes the
-  // state clears them.
+  // but a stage or the host writes it), 2 when moreover the cell kernel
+  // settled the tile to h = hu = hv = +0 without computing it (below).
+  // The cell kernel writes odry_out with the state; the face kernel reads
+  // odry_in.  Whoever else writes the state clears them.
   const int* odry_in;
   int* odry_out;
 };
@@ -302,6 +303,7 @@ struct CellsSmem {
   double th[SPY + 2][SPX + 2];
   double red[2][SP_THREADS / 32];
   int dry[3][3];                  // dry flags of the tile's 3 x 3 neighbourhood
+  int prev;                       // the output tile's record as this kernel left it last time
   bool last;
 };
 
@@ -549,9 +551,17 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
   const int lx = t % SPX, ly = t / SPX;
   const int gi = i0 + lx, gj = j0 + ly;
 
-  // the cell's own state is copied first, in flight while the flags and
-  // the limiter are worked out
-  if (gi < W && gj < H) {
+  // Whether the tile could settle (below), from what is known without a
+  // load.  When a quarter or more of the tiles settled in each stage of the
+  // last step (Control::settled counts one in 16, both stages), such a tile
+  // copies its state only once the flags say that it must be computed, so
+  // a settled tile reads nothing; otherwise every tile copies its state at
+  // once, in flight with the flags.
+  const bool canSettle = !ticket && s.odry_out && s.dry && a.dryfold && a.minDepth >= 0 && a.sponge_width <= 0 &&
+                         !a.h0c && !a.tape_th && !a.tape_hpre && !a.tape_pre[0] &&
+                         i0 >= 2 && i0 + SPX <= W - 2 && j0 >= 2 && j0 + SPY <= H - 2;
+  const bool defer = canSettle && 32 * ctl->settled >= nparts;   // uniform across the grid
+  if (!defer && gi < W && gj < H) {
     const int k = gj * W + gi;
     cp_async8(&sm.st[0][t], a.h + k);
     cp_async8(&sm.st[1][t], a.hu + k);
@@ -562,7 +572,6 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
       cp_async8(&sm.st[5][t], a.ohv + k);
     }
   }
-
   if (t < 9) {
     const int r = t / 3, c = t - 3 * r, txn = tx - 1 + c, tyn = ty - 1 + r;
     int f = 0;                                    // no flags: nothing is skipped
@@ -576,6 +585,48 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
   const bool allDry = sm.dry[0][0] & sm.dry[0][1] & sm.dry[0][2] & sm.dry[1][0] & sm.dry[1][1] &
                       sm.dry[1][2] & sm.dry[2][0] & sm.dry[2][1] & sm.dry[2][2];
   const bool fold = allDry && a.dryfold;          // uniform across the CTA
+  // A folded tile settles without its state.  Its input has h = +-0 on the
+  // tile (the flags), and so does U0 in stage 2 (the output record, which
+  // describes U0 as this kernel wrote it in the previous step).  Every face
+  // and source term is +0 (the fold), so stage 1 gives h = +-0 + dt * (+0)
+  // and stage 2 h = 0.5 ((+-0 + +-0) + dt * (+0)): both +0 for dt > 0.
+  // dryClean then sets hu = hv = +0 (h <= minDepth when minDepth >= 0), as
+  // does friction; with no sponge nothing else writes the cell, the CFL
+  // rate and the floored mass get nothing, and h = +0 never floors.  All
+  // cells are interior (ghost-free tile).  So the tile's output is exactly
+  // (+0, +0, +0), and when the record says the tile already holds that (2)
+  // nothing is written at all.  The tape and the U0 copy need the values:
+  // not with them.
+  if (canSettle && fold && dt > 0 && dt < INFINITY) {   // uniform; only folded tiles read the record
+    if (t == 0) sm.prev = s.odry_out[ty * s.ntx + tx];
+    __syncthreads();
+    if (MODE == 1 || sm.prev >= 1) {
+      if (!defer) cp_async_wait_all();            // the copies of U0 read what is written next
+      if (sm.prev != 2 && gi < W && gj < H) {
+        const int k = gj * W + gi;
+        a.oh[k] = 0.0; a.ohu[k] = 0.0; a.ohv[k] = 0.0;
+      }
+      if (t == 0) {                               // no cell contributes: +0 and 0 (the reduction's result)
+        s.odry_out[ty * s.ntx + tx] = 2;
+        if (MODE == 1) a.part_fl1[part] = 0;
+        else { a.part_max[part] = 0; a.part_fl2[part] = 0; }
+        if ((part & 15) == 0) atomicAdd(&ctl->settled_next, 1);
+      }
+      return;                                     // canSettle excludes the ticket
+    }
+  }
+  // the cell's own state, in flight while the limiter is worked out
+  if (defer && gi < W && gj < H) {
+    const int k = gj * W + gi;
+    cp_async8(&sm.st[0][t], a.h + k);
+    cp_async8(&sm.st[1][t], a.hu + k);
+    cp_async8(&sm.st[2][t], a.hv + k);
+    if (MODE == 2) {
+      cp_async8(&sm.st[3][t], a.oh + k);
+      cp_async8(&sm.st[4][t], a.ohu + k);
+      cp_async8(&sm.st[5][t], a.ohv + k);
+    }
+  }
   if (!fold) {
     for (int q = t; q < (SPX + 2) * (SPY + 2); q += SP_THREADS) {
       const int ly = q / (SPX + 2), lx = q - ly * (SPX + 2);
