@@ -96,10 +96,19 @@ struct swe_sim {
   int* d_odry[2] = {nullptr, nullptr};             // per tile of A / B: all h == 0 (swe_split.cuh)
   swe::SplitBufs sb;
   dim3 sgrid;
-  cudaGraphExec_t gexec = nullptr;
-  int g_steps = 0, g_mode = -1;
-  double g_dt = 0, g_tend = 0;
-  unsigned long long g_version = 0, version = 1;
+  // Whether the tiled cell kernels may settle dry tiles (swe_split.cuh):
+  // swe_run keeps it on after its first chunk of steps only when a quarter
+  // or more of the tiles settled there; grids with little dry land run the
+  // plain kernel faster.  The single-step entry points always settle.
+  int settle = 1;
+  // device-resident loop graphs, one per value of `settle`
+  struct LoopGraph {
+    cudaGraphExec_t exec = nullptr;
+    int steps = 0, mode = -1;
+    double dt = 0, tend = 0;
+    unsigned long long version = 0;
+  } graphs[2];
+  unsigned long long version = 1;
 };
 
 namespace {
@@ -330,7 +339,8 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
     sb.odry_out = s->d_odry[MODE == 1 ? 1 : 0];
     const dim3 blk(swe::SP_THREADS);
     CU(launch(pdl, swe::k_split_faces, s->sgrid, blk, s->st, a, sb, s->d_ctl));
-    CU(launch(pdl, swe::k_split_cells<MODE>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
+    if (s->settle) CU(launch(pdl, swe::k_split_cells<MODE, true>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
+    else CU(launch(pdl, swe::k_split_cells<MODE, false>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
     CU(launch(pdl, swe::k_split_close<MODE>, dim3(1), blk, s->st, a, s->d_ctl, (int)(s->sgrid.x * s->sgrid.y)));
   } else {
     swe::k_stage<MODE><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a, s->d_ctl);
@@ -441,7 +451,7 @@ int upload_geom(swe_sim* s) {
 }
 
 void free_all(swe_sim* s) {
-  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  for (auto& g : s->graphs) if (g.exec) cudaGraphExecDestroy(g.exec);
   double** ptrs[] = {&s->d_b, &s->d_A[0], &s->d_A[1], &s->d_A[2], &s->d_B[0], &s->d_B[1], &s->d_B[2],
                      &s->d_h0[0], &s->d_h0[1], &s->d_h0[2], &s->d_res[0], &s->d_res[1], &s->d_res[2],
                      &s->d_res[3], &s->d_nfield, &s->d_geom, &s->d_part, &s->d_rows, &s->d_sponge,
@@ -853,30 +863,57 @@ int swe_run(swe_sim* s, int n, double dt_fixed, double t_end, int* done) {
   const int mode = dt_fixed > 0 ? 2 : 3;
   const double dtv = dt_fixed > 0 ? dt_fixed : 0;
   const int chunk = std::min(n, 32);
-  if (!s->gexec || s->g_steps != chunk || s->g_mode != mode || s->g_dt != dtv || s->g_tend != t_end ||
-      s->g_version != s->version) {
-    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
-    cudaGraph_t graph;
-    CU(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-    for (int q = 0; q < chunk; q++) {
-      rc = enqueue_step(s, mode, dtv, t_end);
-      if (rc) { cudaStreamEndCapture(s->st, &graph); return rc; }
+  // The graph of `chunk` steps with the current value of s->settle, built
+  // once per (chunk, mode, dt, tEnd, options) and kept.
+  auto graph_for = [&](cudaGraphExec_t* out) -> int {
+    swe_sim::LoopGraph& g = s->graphs[s->settle ? 1 : 0];
+    if (!g.exec || g.steps != chunk || g.mode != mode || g.dt != dtv || g.tend != t_end || g.version != s->version) {
+      if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
+      cudaGraph_t graph;
+      CU(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+      for (int q = 0; q < chunk; q++) {
+        const int rq = enqueue_step(s, mode, dtv, t_end);
+        if (rq) { cudaStreamEndCapture(s->st, &graph); return rq; }
+      }
+      CU(cudaStreamEndCapture(s->st, &graph));
+      const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return fail(SWE_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      g.steps = chunk; g.mode = mode; g.dt = dtv; g.tend = t_end; g.version = s->version;
     }
-    CU(cudaStreamEndCapture(s->st, &graph));
-    const cudaError_t e = cudaGraphInstantiate(&s->gexec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return fail(SWE_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-    s->g_steps = chunk; s->g_mode = mode; s->g_dt = dtv; s->g_tend = t_end; s->g_version = s->version;
-  }
+    *out = g.exec;
+    return SWE_OK;
+  };
   int left = n;
+  cudaGraphExec_t exec = nullptr;
+  if (s->stage_impl == 1 && s->d_odry[0]) {
+    // the first chunk settles what it can; the settled-tile count of its
+    // last step decides whether the rest does
+    s->settle = 1;
+    rc = graph_for(&exec);
+    if (rc) return rc;
+    CU(cudaGraphLaunch(exec, s->st));
+    left -= chunk;
+    if (left > 0) {
+      int counted = 0;
+      CU(cudaMemcpyAsync(&counted, &s->d_ctl->settled_next, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+      CU(cudaStreamSynchronize(s->st));
+      s->settle = 32 * counted >= (int)(s->sgrid.x * s->sgrid.y) ? 1 : 0;
+    }
+  }
+  if (left >= chunk) {
+    rc = graph_for(&exec);
+    if (rc) return rc;
+  }
   while (left >= chunk) {
-    CU(cudaGraphLaunch(s->gexec, s->st));
+    CU(cudaGraphLaunch(exec, s->st));
     left -= chunk;
   }
   for (int q = 0; q < left; q++) {
     rc = enqueue_step(s, mode, dtv, t_end);
     if (rc) return rc;
   }
+  s->settle = 1;
   s->clock_valid = false;
   s->cfl_valid = true;
   rc = sync_clock(s);

@@ -54,9 +54,11 @@ struct Control {
   double fl_eta[4], fl_u[4];
   double diag;          // last diagnostic result
   int stop;             // 1: the prepared step was refused (dt not > 0 or not finite)
+  // tiles the tiled cell kernels settled in the last step, one in 16
+  // counted; beside `stop` and `dt`, in the line every kernel reads first
+  int settled;
   int status;           // sticky status bits (1: non-finite CFL rate seen)
   unsigned int counter; // last-CTA ticket
-  int settled;          // tiles the tiled cell kernels settled in the last step, one in 16 counted
   // Flather tide tables (src/tide.mjs:103-107), per side
   int tide_n[4];
   double tide_msl[4], tide_ucoef[4];

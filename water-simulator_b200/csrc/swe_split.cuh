@@ -540,7 +540,9 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
 // partial slot `part` of the `nparts` of its grid.  With `ticket`, the last
 // tile of the grid to finish closes the step; without, the step is closed
 // by k_split_close after the launch.  Every thread of the CTA calls it.
-template <int MODE>
+// SETTLE: tiles may settle (below); without it the function is the plain
+// tile update, which grids with little dry land run faster.
+template <int MODE, bool SETTLE = false>
 __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const SplitBufs& s, Control* ctl, int tx,
                                                  int ty, int part, int nparts, CellsSmem& sm, bool ticket) {
   static_assert(MODE == 1 || MODE == 2, "stages only");
@@ -557,7 +559,7 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
   // copies its state only once the flags say that it must be computed, so
   // a settled tile reads nothing; otherwise every tile copies its state at
   // once, in flight with the flags.
-  const bool canSettle = !ticket && s.odry_out && s.dry && a.dryfold && a.minDepth >= 0 && a.sponge_width <= 0 &&
+  const bool canSettle = SETTLE && !ticket && s.odry_out && s.dry && a.dryfold && a.minDepth >= 0 && a.sponge_width <= 0 &&
                          !a.h0c && !a.tape_th && !a.tape_hpre && !a.tape_pre[0] &&
                          i0 >= 2 && i0 + SPX <= W - 2 && j0 >= 2 && j0 + SPY <= H - 2;
   const bool defer = canSettle && 32 * ctl->settled >= nparts;   // uniform across the grid
@@ -682,13 +684,13 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
 #ifndef SWE_SPLIT_CELLS_MIN_BLOCKS
 #define SWE_SPLIT_CELLS_MIN_BLOCKS 4
 #endif
-template <int MODE>
+template <int MODE, bool SETTLE = false>
 __global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_CELLS_MIN_BLOCKS)
 k_split_cells(StageArgs a, SplitBufs s, Control* ctl) {
   pdl_enter();
   if (ctl->stop) return;
   __shared__ CellsSmem sm;
-  split_cells_tile<MODE>(a, s, ctl, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
+  split_cells_tile<MODE, SETTLE>(a, s, ctl, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
                          gridDim.x * gridDim.y, sm, false);
 }
 
