@@ -96,11 +96,12 @@ struct swe_sim {
   int* d_odry[2] = {nullptr, nullptr};             // per tile of A / B: all h == 0 (swe_split.cuh)
   swe::SplitBufs sb;
   dim3 sgrid;
-  // Whether the tiled cell kernels may settle dry tiles (swe_split.cuh):
-  // swe_run keeps it on after its first chunk of steps only when a quarter
-  // or more of the tiles settled there; grids with little dry land run the
-  // plain kernel faster.  The single-step entry points always settle.
-  int settle = 1;
+  // Whether the tiled cell kernels may settle dry tiles (swe_split.cuh).
+  // A swe_run of 128 steps or more keeps it on after its first chunk only
+  // when a quarter or more of the tiles settled there, and remembers the
+  // choice (settle_pref) for shorter runs; grids with little dry land run
+  // the plain kernel faster.  The single-step entry points always settle.
+  int settle = 1, settle_pref = 1;
   // device-resident loop graphs, one per value of `settle`
   struct LoopGraph {
     cudaGraphExec_t exec = nullptr;
@@ -886,9 +887,10 @@ int swe_run(swe_sim* s, int n, double dt_fixed, double t_end, int* done) {
   };
   int left = n;
   cudaGraphExec_t exec = nullptr;
-  if (s->stage_impl == 1 && s->d_odry[0]) {
+  s->settle = s->settle_pref;
+  if (s->stage_impl == 1 && s->d_odry[0] && n >= 4 * chunk) {
     // the first chunk settles what it can; the settled-tile count of its
-    // last step decides whether the rest does
+    // last step decides whether the rest (and later short runs) do
     s->settle = 1;
     rc = graph_for(&exec);
     if (rc) return rc;
@@ -898,7 +900,7 @@ int swe_run(swe_sim* s, int n, double dt_fixed, double t_end, int* done) {
       int counted = 0;
       CU(cudaMemcpyAsync(&counted, &s->d_ctl->settled_next, sizeof(int), cudaMemcpyDeviceToHost, s->st));
       CU(cudaStreamSynchronize(s->st));
-      s->settle = 32 * counted >= (int)(s->sgrid.x * s->sgrid.y) ? 1 : 0;
+      s->settle = s->settle_pref = 32 * counted >= (int)(s->sgrid.x * s->sgrid.y) ? 1 : 0;
     }
   }
   if (left >= chunk) {
