@@ -129,6 +129,13 @@ int swe_get_dims(swe_sim* s, int* dims4);
 /* sim.b / sim.h / ... reads and writes (src/swe.mjs:200-220). */
 int swe_get_field(swe_sim* s, int field, double* out);
 int swe_set_field(swe_sim* s, int field, const double* in);
+/* Rows [row0, row0 + nrows) of the padded grid (row-major, W doubles per
+ * row) of b, h, hu or hv: the halo exchange of a grid cut into row slabs
+ * (water-simulator_b200/slabs.py).  No counterpart in the reference, which
+ * runs one grid on one thread (src/swe.mjs:968-973).  Writing h, hu or hv
+ * clears the dry-tile records, as swe_set_field does. */
+int swe_get_rows(swe_sim* s, int field, int row0, int nrows, double* out);
+int swe_set_rows(swe_sim* s, int field, int row0, int nrows, const double* in);
 /* sim.geom.* rows (src/geometry.mjs:301-309); writes take effect from the
  * next device call, as a JS write to geom rows does (tools/verify-sphere.mjs:569). */
 int swe_get_geom(swe_sim* s, int row, double* out);

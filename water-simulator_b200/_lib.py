@@ -68,6 +68,8 @@ SIGNATURES = {
     "swe_get_dims": [_P, _IP],
     "swe_get_field": [_P, _I, _DP],
     "swe_set_field": [_P, _I, _DP],
+    "swe_get_rows": [_P, _I, _I, _I, _DP],
+    "swe_set_rows": [_P, _I, _I, _I, _DP],
     "swe_get_geom": [_P, _I, _DP],
     "swe_set_geom": [_P, _I, _DP],
     "swe_get_scalar": [_P, _I, _DP],

@@ -606,6 +606,31 @@ int swe_set_field(swe_sim* s, int field, const double* in) {
   return SWE_OK;
 }
 
+int swe_get_rows(swe_sim* s, int field, int row0, int nrows, double* out) {
+  if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  if (field != SWE_FIELD_B && field != SWE_FIELD_H && field != SWE_FIELD_HU && field != SWE_FIELD_HV)
+    return fail(SWE_EINVAL, "swe_get_rows: b, h, hu or hv");
+  if (row0 < 0 || nrows < 0 || row0 > s->H - nrows) return fail(SWE_EINVAL, "swe_get_rows: rows out of range");
+  if (nrows == 0) return SWE_OK;
+  const size_t off = (size_t)row0 * s->W, nb = sizeof(double) * (size_t)nrows * s->W;
+  CU(cudaMemcpyAsync(out, field_ptr(s, field) + off, nb, cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  return SWE_OK;
+}
+
+int swe_set_rows(swe_sim* s, int field, int row0, int nrows, const double* in) {
+  if (!s || !in) return fail(SWE_EINVAL, "null argument");
+  if (field != SWE_FIELD_B && field != SWE_FIELD_H && field != SWE_FIELD_HU && field != SWE_FIELD_HV)
+    return fail(SWE_EINVAL, "swe_set_rows: b, h, hu or hv");
+  if (row0 < 0 || nrows < 0 || row0 > s->H - nrows) return fail(SWE_EINVAL, "swe_set_rows: rows out of range");
+  if (nrows == 0) return SWE_OK;
+  const size_t off = (size_t)row0 * s->W, nb = sizeof(double) * (size_t)nrows * s->W;
+  CU(cudaMemcpyAsync(field_ptr(s, field) + off, in, nb, cudaMemcpyHostToDevice, s->st));
+  if (field != SWE_FIELD_B && forget_dry(s)) return SWE_ECUDA;
+  s->cfl_valid = false;
+  return SWE_OK;
+}
+
 int swe_get_geom(swe_sim* s, int row, double* out) {
   if (!s || !out) return fail(SWE_EINVAL, "null argument");
   if (row < 0 || row >= SWE_GEOM_NROWS) return fail(SWE_EINVAL, "unknown metric row id");

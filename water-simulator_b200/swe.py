@@ -382,6 +382,23 @@ class ShallowWater:
     rhv = property(lambda s: s._writable("rhv"))
     theta = property(lambda s: s._writable("theta"))
 
+    def get_rows(self, name, row0, nrows):
+        """Rows [row0, row0 + nrows) of b, h, hu or hv over the padded grid,
+        read from the device (the halo exchange of slabs.py)."""
+        self._push()
+        out = np.empty(int(nrows) * self.W)
+        check(self._lib.swe_get_rows(self._h, FIELD[name], int(row0), int(nrows), dptr(out)))
+        return out
+
+    def set_rows(self, name, row0, values):
+        """Write rows starting at row0 of b, h, hu or hv on the device."""
+        self._push()
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        if v.size % self.W:
+            raise ValueError("set_rows: a whole number of rows of W values")
+        check(self._lib.swe_set_rows(self._h, FIELD[name], int(row0), v.size // self.W, dptr(v)))
+        self._stale(name)
+
     def _h0(self, name):
         if not self._keep_h0:
             check(self._lib.swe_set_keep_h0(self._h, 1))
