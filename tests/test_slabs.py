@@ -190,3 +190,89 @@ def test_local_slabs_match_one_grid_on_the_gpu():
             assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), (step, f)
     for sim in run.sims + [whole]:
         sim.close()
+
+
+# ---- a spherical band: every row has its own metric ------------------------
+SNX, SNY, LAT0, LAT1 = 36, 48, -60.0, 60.0
+SPHERE = {"R": 6371e3, "lat0": LAT0, "lat1": LAT1, "omega": 7.2921e-5}
+
+
+def sphere_case():
+    """Still water 0-4000 m deep over a bed with a continent (land at +50 m)
+    in the northern slab, a released hump across the southern cut, Coriolis
+    on; walls at the band's edges, longitude periodic."""
+    W, H = SNX + 4, SNY + 4
+    lon = (np.arange(W) - 2 + 0.5) * (360.0 / SNX)
+    lat = LAT0 + (np.arange(H) - 2 + 0.5) * ((LAT1 - LAT0) / SNY)
+    L, P = np.meshgrid(lon, lat)
+    b = -4000.0 + 1500.0 * np.sin(np.radians(2 * L)) * np.cos(np.radians(3 * P))
+    b = np.where((P > 25) & (L > 60) & (L < 140), 50.0, b)
+    eta = 2.0 * np.exp(-((L - 200.0) ** 2 + (P + 20.0) ** 2) / 200.0)
+    return b, eta
+
+
+def sphere_bounds(**extra):
+    return dict(west="periodic", east="periodic", south="reflect", north="reflect", **extra)
+
+
+def band(slab):
+    dphi = (LAT1 - LAT0) / SNY
+    return dict(SPHERE, lat0=LAT0 + slab.e0 * dphi, lat1=LAT0 + slab.e1 * dphi)
+
+
+def test_local_slabs_match_one_sphere_on_the_oracle():
+    sl = _slabs()
+    b, eta = sphere_case()
+    whole = OracleRows(nx=SNX, ny=SNY, bed=b, eta0=eta, sphere=SPHERE, manning=0.025)
+    whole.sim.set_boundaries(**sphere_bounds())
+    slabs = [sl.Slab(SNY, a, c) for a, c in sl.slab_rows(SNY, 3)]
+    sims = []
+    for s in slabs:
+        o = OracleRows(nx=SNX, ny=s.rows, bed=s.take(b), eta0=s.take(eta), sphere=band(s), manning=0.025)
+        o.sim.set_boundaries(**sphere_bounds())
+        sl.copy_geometry(o.sim, s, whole.sim.geom)
+        sims.append(o)
+    run = sl.LocalSlabs(slabs, sims)
+    for _ in range(STEPS):
+        dt = run.step()
+        assert whole.maxDt() == dt
+        whole.step(dt)
+    for f in ("h", "hu", "hv"):
+        want = whole.get_rows(f, 2, SNY).reshape(SNY, -1)
+        assert np.array_equal(run.gather(f).view(np.uint64), want.view(np.uint64)), f
+    hv = want  # the last field gathered: hv
+    assert np.all(hv[14:34, 2:-2] != 0)                     # motion across both cuts (rows 16 and 32)
+    assert np.count_nonzero(whole.get_rows("h", 2, SNY) == 0) > 0      # the continent stays dry
+
+
+@pytest.mark.gpu
+def test_local_slabs_match_one_sphere_on_the_gpu():
+    """Three slab handles of a spherical band, each given the band's own
+    metric rows, against one handle of the whole band after every step."""
+    sl = _slabs()
+    import __graft_entry__
+    swe = __graft_entry__.load_package()
+    b, eta = sphere_case()
+
+    def make(ny, bb, ee, sphere):
+        sim = swe.ShallowWater(nx=SNX, ny=ny, bed=bb, eta0=ee, sphere=sphere, manning=0.025)
+        sim.boundaries = {"west": swe.periodic, "east": swe.periodic, "south": swe.reflect, "north": swe.reflect}
+        return sim
+
+    whole = make(SNY, b, eta, SPHERE)
+    slabs = [sl.Slab(SNY, a, c) for a, c in sl.slab_rows(SNY, 3)]
+    sims = []
+    for s in slabs:
+        sim = make(s.rows, s.take(b), s.take(eta), band(s))
+        sl.copy_geometry(sim, s, whole.geom)
+        sims.append(sim)
+    run = sl.LocalSlabs(slabs, sims)
+    for step in range(STEPS):
+        dt = run.step()
+        assert whole.maxDt() == dt
+        whole.step(dt)
+        for f in ("h", "hu", "hv"):
+            want = whole.get_rows(f, 2, SNY).reshape(SNY, -1)
+            assert np.array_equal(run.gather(f).view(np.uint64), want.view(np.uint64)), (step, f)
+    for sim in run.sims + [whole]:
+        sim.close()

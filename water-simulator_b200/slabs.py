@@ -18,6 +18,11 @@ rows (owned + halo) hold the single grid's state, so the smallest of the
 slabs' own maxDt() is cfl over the global largest rate, the same double
 (cfl / x decreases with x and is correctly rounded).
 
+On a spherical grid the metric differs row by row: a slab's simulation
+takes the grid's own 13 metric rows over its padded rows (`copy_geometry`),
+so that its arithmetic is the grid's, not that of a band recomputed from
+its latitudes.
+
 Limits: the global south and north boundaries may not be periodic (they
 would wrap the slabs), and massFloored, volume() and the other
 diagnostics of a slab count its halo rows too; take them from the owned
@@ -82,6 +87,19 @@ class Slab:
 
     def recv_north(self):
         return self.b - self.e0 + 2, self.e1 - self.b
+
+
+GEOM_ROWS = ("dxRow", "dyRowN", "dyRowS", "dyCFL", "area", "lx", "lyN", "lyS", "bedPhi", "phiC", "tanPhi",
+             "fRow", "geoCoef")
+
+
+def copy_geometry(sim, slab, grid_geom):
+    """Give a slab's simulation the grid's metric rows over the slab's padded
+    rows (src/geometry.mjs:301-309); `grid_geom` is the grid's geometry
+    object (or a mapping of row name to array)."""
+    for name in GEOM_ROWS:
+        full = grid_geom[name] if isinstance(grid_geom, dict) else getattr(grid_geom, name)
+        getattr(sim.geom, name)[:] = np.asarray(full, dtype=np.float64)[slab.e0:slab.e1 + 4]
 
 
 FIELDS = ("h", "hu", "hv")
