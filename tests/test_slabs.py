@@ -27,8 +27,8 @@ def _slabs():
     return slabs
 
 
-def case():
-    W, H = NX + 4, NY + 4
+def case(ny=NY):
+    W, H = NX + 4, ny + 4
     rng = np.random.default_rng(5)
     y = (np.arange(H) - 2 + 0.5) * DX
     x = (np.arange(W) - 2 + 0.5) * DX
@@ -77,13 +77,13 @@ def oracle_grid(ny, b, eta):
     return o
 
 
-def reference_rows(steps=STEPS):
+def reference_rows(steps=STEPS, ny=NY):
     """The grid itself on the oracle: its interior rows after `steps` and t."""
-    b, eta = case()
-    ref = oracle_grid(NY, b, eta)
+    b, eta = case(ny)
+    ref = oracle_grid(ny, b, eta)
     for _ in range(steps):
         ref.step(ref.maxDt())
-    out = {f: ref.get_rows(f, 2, NY).reshape(NY, -1) for f in ("h", "hu", "hv")}
+    out = {f: ref.get_rows(f, 2, ny).reshape(ny, -1) for f in ("h", "hu", "hv")}
     return out, ref.sim.t
 
 
@@ -121,6 +121,23 @@ def test_local_slabs_match_one_grid_on_the_oracle():
     hv = want["hv"][:, 2:-2]
     assert np.all(hv[14:46] != 0)
     assert np.count_nonzero(want["h"][NY - 4:, 2:-2] == 0) > 0
+
+
+def test_slabs_as_short_as_the_halo():
+    """Four slabs of 6 rows: each halo is a whole neighbouring slab, and the
+    inner slabs' halos reach the grid's own walls."""
+    sl = _slabs()
+    ny = 24
+    b, eta = case(ny)
+    want, t_want = reference_rows(ny=ny)
+    slabs = [sl.Slab(ny, a, c) for a, c in sl.slab_rows(ny, 4)]
+    assert [s.b - s.a for s in slabs] == [6, 6, 6, 6]
+    run = sl.LocalSlabs(slabs, [oracle_grid(s.rows, s.take(b), s.take(eta)) for s in slabs])
+    for _ in range(STEPS):
+        run.step()
+    for f in ("h", "hu", "hv"):
+        assert np.array_equal(run.gather(f).view(np.uint64), want[f].view(np.uint64)), f
+    assert all(s.sim.t == t_want for s in run.sims)
 
 
 def _rank_main(rank, world, port, out_dir):
