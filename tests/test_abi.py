@@ -89,3 +89,15 @@ def test_no_device_fails_loudly(swe):
     """No CPU fallback: without a CUDA device the constructor raises."""
     with pytest.raises(swe.SweError, match="no CUDA device"):
         swe.ShallowWater(nx=8, ny=8, dx=1, bed=lambda x, y: 0, eta0=1)
+
+
+def test_row_access_refuses_bad_arguments_without_a_device(swe):
+    """swe_get_rows / swe_set_rows (the row slabs' halo exchange) check
+    their arguments before any device call."""
+    lib = swe.load_library()
+    from water_simulator_b200 import _lib
+    buf = np.zeros(16)
+    ptr = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert lib.swe_get_rows(None, _lib.FIELD["h"], 0, 1, ptr) == _lib.SWE_EINVAL
+    assert lib.swe_set_rows(None, _lib.FIELD["h"], 0, 1, ptr) == _lib.SWE_EINVAL
+    assert b"null" in lib.swe_last_error()
