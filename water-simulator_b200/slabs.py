@@ -163,7 +163,9 @@ class DistributedSlab:
     """This rank's slab of a grid cut over the ranks of a torch.distributed
     group (rank k holds slab k): halos go to the neighbours by point-to-point
     messages, dt is the minimum of the ranks' maxDt() (all_reduce MIN).
-    `device` is where the messages live: "cpu" for gloo, "cuda" for NCCL."""
+    `device` is where the messages live: "cpu" for gloo, "cuda" for NCCL.
+    On several GPUs each rank makes its slab's simulation on its own device
+    (`swe_set_device(local rank)` before the handle is created)."""
 
     def __init__(self, slab, sim, dist, group=None, device="cpu"):
         self.slab, self.sim, self.dist, self.group, self.device = slab, sim, dist, group, device
