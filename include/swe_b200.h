@@ -136,6 +136,21 @@ int swe_set_field(swe_sim* s, int field, const double* in);
  * clears the dry-tile records, as swe_set_field does. */
 int swe_get_rows(swe_sim* s, int field, int row0, int nrows, double* out);
 int swe_set_rows(swe_sim* s, int field, int row0, int nrows, const double* in);
+/* The same row copies without a host synchronisation, for a halo exchange
+ * that stays on the device: dst / src may be device memory (another
+ * buffer, a peer GPU's, a collective's) or pinned host memory.  They are
+ * ordered on the handle's stream (swe_get_stream); the caller keeps src
+ * valid until the stream has reached the copy. */
+int swe_get_rows_async(swe_sim* s, int field, int row0, int nrows, double* dst);
+int swe_set_rows_async(swe_sim* s, int field, int row0, int nrows, const double* src);
+/* maxDt() written to the device double *dst on the handle's stream (no host
+ * round trip), and step(dt) with dt read from the device double *dt when
+ * the step runs: a grid cut into slabs over GPUs all-reduces the slabs'
+ * maxDt on the device and steps each slab with the result.  A dt that is
+ * not > 0 or not finite makes the step change nothing, as in swe_run.  No
+ * counterpart in the reference (one grid, one thread, src/swe.mjs:968). */
+int swe_max_dt_to(swe_sim* s, double* dst);
+int swe_step_dt_from(swe_sim* s, const double* dt);
 /* sim.geom.* rows (src/geometry.mjs:301-309); writes take effect from the
  * next device call, as a JS write to geom rows does (tools/verify-sphere.mjs:569). */
 int swe_get_geom(swe_sim* s, int row, double* out);
@@ -187,6 +202,23 @@ int swe_run(swe_sim* s, int n, double dt_fixed, double t_end, int* done);
 int swe_volume(swe_sim* s, double* out);
 int swe_energy(swe_sim* s, double* out);
 int swe_max_surface_deviation(swe_sim* s, double ref, double* out);
+/* The order of the Cartesian volume() sum.  SWE_DIAG_REFERENCE (the
+ * default): one running sum over every interior cell in row-major order,
+ * then one multiply by dx and dy -- the reference's own order
+ * (src/swe.mjs:818-827) and its bits, but a chain of nx*ny dependent
+ * additions.  SWE_DIAG_ROWS: each row summed left to right, then the rows
+ * in order (the order the sphere's volume uses), then dx and dy: the same
+ * result to round-off, deterministic, and parallel over rows.  Every other
+ * diagnostic is in the reference's order and parallel already. */
+#define SWE_DIAG_REFERENCE 0
+#define SWE_DIAG_ROWS      1
+int swe_set_diag_order(swe_sim* s, int order);
+/* The area-weighted projection measureModePeriod() samples after every
+ * step (src/globe.mjs:1414-1421): sum over interior rows j, in order, of
+ * coef[j] * (sum over the row, left to right, of b + h), with coef[j] =
+ * (wRow[j] / nx) * pRow[j] formed by the caller (ny doubles).  The same
+ * bits as the reference's loop, and 8 bytes to the host per call. */
+int swe_eta_projection(swe_sim* s, const double* coef, double* out);
 int swe_max_speed(swe_sim* s, double* out);
 int swe_finite(swe_sim* s, int* out);
 int swe_synchronize(swe_sim* s);
@@ -238,7 +270,25 @@ int swe_batch_get_schedule(swe_batch* s, int* out4);
 int swe_batch_autotune(swe_batch* s, int trial_steps, int* best4, double* best_ms_per_step);
 /* `steps` ensemble steps: every basin takes `steps` steps of its own maxDt(). */
 int swe_batch_run(swe_batch* s, int steps);
+/* Waits for the ensemble's stream; SWE_ETIMEOUT (once, then cleared) when a
+ * work-queue wait of the steps run since the last call ran past its limit. */
 int swe_batch_synchronize(swe_batch* s);
+/* The launch form of an ensemble step with the tiled pair (rows 0).
+ * 0: a launch per phase (prepare, ghost fill, faces, cells, ghost fill,
+ * faces, cells).  1: ONE persistent launch per step over a device work
+ * queue of every (basin, phase, tile) item in phase order; a CTA takes the
+ * next item and waits, with a time limit, until the previous phase of that
+ * item's basin is complete.  A wait past its limit drops the rest of the
+ * step and swe_batch_synchronize returns SWE_ETIMEOUT.  Results are the same
+ * bits either way.  The autotuner tries both. */
+int swe_batch_set_launch(swe_batch* s, int queue);
+int swe_batch_get_launch(swe_batch* s, int* queue);
+/* The time limit of one work-queue wait (default 2 s). */
+int swe_batch_set_wait_limit(swe_batch* s, double seconds);
+/* Test hook: the prepare of `basin` is never marked complete (-1: none), so
+ * that basin's next phase waits until its limit -- a wait that nothing
+ * ends, for checking that it does end, with SWE_ETIMEOUT. */
+int swe_batch_debug_hold(swe_batch* s, int basin);
 int swe_batch_get_stream(swe_batch* s, void** stream);
 int swe_batch_get_field(swe_batch* s, int basin, int field, double* out);   /* B, H, HU, HV */
 int swe_batch_get_scalar(swe_batch* s, int basin, int which, double* out);  /* T, STEPS, MASS_FLOORED */
@@ -267,18 +317,6 @@ int swe_adjoint_backward(swe_adjoint* s, double* grad_b, double* grad_n);
 int swe_adjoint_dt_sequence(swe_adjoint* s, double* dts_out, const double* dts_in);
 int swe_adjoint_get_stream(swe_adjoint* s, void** stream);
 
-/* maxDt() for callers that cannot allocate device memory.  It has no
- * counterpart in the reference; it serves callers that own all device memory
- * themselves (a fixed arena, a hard memory cap, a region where allocation is
- * forbidden) and so cannot create a handle.  Inputs are the caller's device
- * arrays over the padded grid (h, hu, hv: (nx+4)*(ny+4) doubles; dx_row,
- * dy_cfl: ny+4 doubles, the metric rows of src/geometry.mjs); the result,
- * cfl / max rate or Infinity, is written to the device double *dt_out, in
- * `stream` (a cudaStream_t, NULL for the default stream).  It allocates
- * nothing: its reduction scratch is a fixed array inside the library, so
- * ny is limited to SWE_NOALLOC_MAX_ROWS (larger grids get SWE_EINVAL), calls
- * that overlap on the GPU race, and the first call on each device looks the
- * array up and should come before any stream capture. */
 /* ---- stage kernels -----------------------------------------------------------
  * Two implementations of each SSP-RK2 stage, bit-identical in their results:
  * SWE_STAGE_FUSED, one row-marching kernel per stage that keeps the stencil
@@ -329,6 +367,15 @@ int swe_gridlands_decode(const char* b64, size_t len, int n, float* out);
  * setManningField() refuses it. */
 int swe_gridlands_create(const swe_options* o, const swe_gridlands* g, swe_sim** out);
 
+/* The connected waterbodies of waterbodies() (src/gridlands.mjs:107-139) as
+ * a device pass: label[k] (W*H ints, host) is, for a wet cell
+ * (surface - bed > 0), the lowest cell index of its 4-connected wet body --
+ * the cell the reference's row-major flood fill starts that body from --
+ * and -1 for a dry cell.  bed and surface are the export's float32 layers
+ * (host, row 0 first).  SWE_ETIMEOUT if a union failed to settle within its
+ * bounded retries (nothing is left waiting on the device). */
+int swe_gridlands_bodies(int W, int H, const float* bed, const float* surface, int* label);
+
 /* ---- headless frames (src/render.mjs, src/globe.mjs) ------------------------
  * RGBA bytes written into a device buffer (rgba_device, when non-NULL) and/or
  * copied to the host (rgba_host), stored as the reference's ImageData stores
@@ -370,6 +417,20 @@ int swe_globe_lut_get(swe_globe_lut* lut, int* counts, int* px, double* lon_base
 int swe_render_globe(swe_sim* s, swe_globe_lut* lut, double rot_deg, double scale, double msl, int land_light,
                      unsigned char* rgba_host, void* rgba_device, double* stats);
 
+/* maxDt() for callers that cannot allocate device memory.  It has no
+ * counterpart in the reference; it serves callers that own all device memory
+ * themselves (a fixed arena, a hard memory cap, a region where allocation is
+ * forbidden) and so cannot create a handle.  Inputs are the caller's device
+ * arrays over the padded grid (h, hu, hv: (nx+4)*(ny+4) doubles; dx_row,
+ * dy_cfl: ny+4 doubles, the metric rows of src/geometry.mjs); the result,
+ * cfl / max rate or Infinity, is written to the device double *dt_out, in
+ * `stream` (a cudaStream_t, NULL for the default stream).  It allocates
+ * nothing: its reduction scratch is a fixed array inside the library, so
+ * ny is limited to SWE_NOALLOC_MAX_ROWS (larger grids get SWE_EINVAL), calls
+ * that overlap on the GPU race, and the first call on each device looks the
+ * array up and should come before any stream capture.  The looked-up
+ * address belongs to the device's context: after cudaDeviceReset() the
+ * entry point must not be called again in the same process. */
 #define SWE_NOALLOC_MAX_ROWS 16384
 int swe_max_dt_noalloc(int nx, int ny, const double* h, const double* hu, const double* hv,
                        const double* dx_row, const double* dy_cfl, double min_depth, double cfl,

@@ -9,18 +9,20 @@ Sources, all inside Syntaxswine/water-simulator:
   tools/verify-physics.mjs       the positivity factor the solver returns in the
                                  one-wet-cell rig ("the solver returns 0.6666...")
   README.md (claims table)       closed-basin mass drift over 600 steps
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/the/reference/tree
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_pins.json")
 
 
 def main():
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py /path/to/the/reference/tree")
+    REF = sys.argv[1]
     with open(os.path.join(REF, "tools", "sphere-baseline.json")) as f:
         base = json.load(f)
     with open(os.path.join(REF, "README.md")) as f:

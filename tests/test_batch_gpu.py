@@ -85,3 +85,52 @@ def test_autotune_keeps_state(swe):
         assert np.array_equal(ens.field(q, "h"), ref.field(q, "h"))
     ens.close()
     ref.close()
+
+
+@pytest.mark.parametrize("sched", [dict(rows=0, ctas=0, order=0), dict(rows=0, ctas=148, order=1),
+                                   dict(rows=0, ctas=7, order=2)])
+def test_queue_launch_matches_phase_launches(swe, sched):
+    """One persistent launch per step over the work queue gives every basin
+    the same bits as a launch per phase, for any grid and tile order (a
+    7-CTA grid makes nearly every item wait on the one before it)."""
+    bs = basins(swe)
+    ref = swe.Ensemble(bs)
+    ref.run(23)
+    ens = swe.Ensemble(bs)
+    ens.set_schedule(**sched)
+    ens.set_launch("queue")
+    assert ens.launch == "queue"
+    ens.run(23)
+    ens.synchronize()
+    for q in range(len(bs)):
+        for f in ("h", "hu", "hv"):
+            assert np.array_equal(ens.field(q, f), ref.field(q, f)), (sched, q, f)
+        assert ens.t(q) == ref.t(q) and ens.steps(q) == 23
+    ref.close()
+    ens.close()
+
+
+def test_queue_wait_that_nothing_ends_times_out(swe):
+    """A basin whose prepare is never marked done (the test hook): its next
+    phase waits until the limit (50 ms), the step is dropped, and the host
+    reads SWE_ETIMEOUT; the GPU stays usable and the hook off runs again."""
+    import time
+    bs = basins(swe)
+    ens = swe.Ensemble(bs)
+    ens.set_launch("queue")
+    ens.set_wait_limit(0.05)
+    ens.debug_hold(3)
+    t0 = time.perf_counter()
+    ens.run(2)
+    with pytest.raises(swe.SweError) as e:
+        ens.synchronize()
+    assert e.value.code == -4                          # SWE_ETIMEOUT
+    assert time.perf_counter() - t0 < 30
+    ens.synchronize()                                  # reported once, then cleared
+    ens.close()
+    fresh = swe.Ensemble(bs)
+    fresh.set_launch("queue")
+    fresh.run(3)
+    fresh.synchronize()
+    assert all(fresh.steps(q) == 3 for q in range(len(bs)))
+    fresh.close()

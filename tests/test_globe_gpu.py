@@ -1,0 +1,171 @@
+"""The spherical scenarios of src/globe.mjs (water-simulator_b200/globe.py) on
+the GPU: measureModePeriod against a restatement of the reference's driver
+on the oracle (the same steps, crossings and period, bit for bit), the
+checks of the reference's own `merian` section (src/globe.mjs:2918-2948),
+polarTimestepTax, surveyBed against the dry-cell counts and crests the
+reference records for its seamount (src/globe.mjs:1057-1066), dropBump,
+and the device projection (swe_eta_projection) against the reference's
+summation order."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle_sim import OracleSim
+import scenarios as S
+
+pytestmark = pytest.mark.gpu
+
+G_REF = 9.80665
+R_REF = 6371000.0
+D2R = math.pi / 180
+
+
+def _P(n, x):
+    return {2: 0.5 * (3 * x * x - 1), 3: 0.5 * (5 * x * x * x - 3 * x),
+            4: (35 * x ** 4 - 30 * x * x + 3) / 8}[n]
+
+
+def mode_period_on_oracle(n=2, deg=6, H=4000.0, R=R_REF, gRef=G_REF, amp=1.0, periods=2, cfl=0.45):
+    """src/globe.mjs:1387-1450 restated on the oracle (test infrastructure):
+    the projection summed row by row left to right, rows in order."""
+    nx, ny = round(360 / deg), round(180 / deg)
+    closed = 2 * math.pi * R / math.sqrt(gRef * H * n * (n + 1))
+    sim = OracleSim(nx=nx, ny=ny, bed=lambda lon, lat: -H, manning=0, cfl=cfl,
+                    eta0=lambda lon, lat: amp * _P(n, math.sin(lat * D2R)),
+                    sphere={"R": R, "lat0": -90, "lat1": 90, "omega": 0})
+    area, phi = np.array(sim.geom.area), np.array(sim.geom.phiC)
+    wr, pr, norm = [], [], 0.0
+    for j in range(ny):
+        p = _P(n, math.sin(phi[j + 2]))
+        w = area[j + 2] * nx
+        pr.append(p)
+        wr.append(w)
+        norm += w * p * p
+
+    def project():
+        eta = (sim.field("b") + sim.field("h")).reshape(sim.H, sim.W)[2:-2, 2:-2]
+        s = 0.0
+        for j in range(ny):
+            row = 0.0
+            for v in eta[j]:
+                row += v
+            s += (wr[j] / nx) * pr[j] * row
+        return s / norm
+
+    t_end = periods * closed
+    cross, prev_t, prev_c, steps = [], 0.0, project(), 0
+    while sim.t < t_end:
+        dt = min(sim.maxDt(), t_end - sim.t)
+        if not dt > 0:
+            break
+        sim.step(dt)
+        steps += 1
+        c = project()
+        if (prev_c < 0) != (c < 0):
+            cross.append(prev_t + (sim.t - prev_t) * (0 - prev_c) / (c - prev_c))
+        prev_t, prev_c = sim.t, c
+    sim.close()
+    measured = 2 * (cross[-1] - cross[0]) / (len(cross) - 1)
+    return {"measured": measured, "closed": closed, "steps": steps, "crossings": len(cross)}
+
+
+def test_mode_period_bit_identical_to_the_oracle(swe):
+    from water_simulator_b200 import globe
+    got = globe.measureModePeriod(n=2, deg=6, gRef=G_REF)
+    want = mode_period_on_oracle(n=2, deg=6)
+    assert got["steps"] == want["steps"] and got["crossings"] == want["crossings"]
+    assert got["measured"] == want["measured"]
+    assert got["closed"] == want["closed"]
+
+
+def test_merian_section(swe):
+    """src/globe.mjs:2918-2948: the n = 2 period within 1 % at 6 and 4
+    degrees and late, n = 3 within 1 % and faster by sqrt(n(n+1)), the
+    solver's gravity equal to the test's own, and the refusals."""
+    from water_simulator_b200 import globe
+    assert swe.G == G_REF
+    for deg in (6, 4):
+        r = globe.measureModePeriod(n=2, deg=deg, H=4000, R=R_REF, gRef=G_REF, amp=1, periods=2)
+        assert abs(r["measured"] - r["closed"]) <= 0.01 * r["closed"], r
+        assert r["rel"] < 0, r
+    r3 = globe.measureModePeriod(n=3, deg=6, H=4000, R=R_REF, gRef=G_REF, amp=1, periods=2)
+    assert abs(r3["measured"] - r3["closed"]) <= 0.01 * r3["closed"]
+    assert r3["closed"] < 0.72 * 2 * math.pi * R_REF / math.sqrt(G_REF * 4000 * 2 * 3)
+    with pytest.raises(ValueError, match="gRef is required"):
+        globe.measureModePeriod(n=2, deg=12, R=R_REF)
+    with pytest.raises(ValueError):
+        globe.legendreP(1, 0.3)
+
+
+def test_projection_in_reference_order(swe):
+    """swe_eta_projection gives the reference loop's double on a state with
+    every cell different."""
+    from water_simulator_b200 import globe
+    rng = np.random.default_rng(9)
+    sim = S.sphere(swe.ShallowWater, S.bed_uneven, 4, eta0=lambda lon, lat: 0.0)
+    h = sim.h
+    h[:] = h + rng.uniform(0, 3, h.shape)
+    proj = globe.ModeProjection(sim, 3)
+    got = proj() * proj.norm
+    eta = (sim.field("b") + sim.field("h")).reshape(sim.H, sim.W)[2:-2, 2:-2]
+    want = 0.0
+    for j in range(sim.ny):
+        row = 0.0
+        for v in eta[j]:
+            row += v
+        want += proj.coef[j] * row
+    assert got == want
+    sim.close()
+
+
+def test_polar_timestep_tax(swe):
+    """At 3 degrees the polar row's CFL step is more than 5 times smaller
+    than the equator's (src/globe.mjs:2891-2895); the rows are the metric's."""
+    from water_simulator_b200 import globe
+    sim = swe.ShallowWater(nx=120, ny=60, bed=lambda lon, lat: -4000, eta0=0, manning=0,
+                           sphere={"R": R_REF, "lat0": -90, "lat1": 90, "omega": 0})
+    tax = globe.polarTimestepTax(sim)
+    assert tax["ratio"] > 5
+    g = sim.geom
+    c = math.sqrt(G_REF * 4000)
+    dts = [sim.cfl / (c / g._rows["dxRow"][j] + c / g._rows["dyCFL"][j]) for j in range(2, sim.ny + 2)]
+    assert tax["pole"] == min(dts)
+    assert abs(abs(tax["poleLat"]) - 88.5) < 1e-9 and abs(abs(tax["eqLat"]) - 1.5) < 1e-9
+    with pytest.raises(ValueError):
+        globe.polarTimestepTax(swe.ShallowWater(nx=4, ny=4, dx=1, bed=lambda x, y: -1, eta0=0))
+    sim.close()
+
+
+@pytest.mark.parametrize("deg,dry,crest", [(4, 16, 1095), (3, 36, None), (2, 80, 1173)])
+def test_survey_bed_of_the_seamount(swe, deg, dry, crest):
+    """The reference records its seamount's dry cells (16 at 4 deg, 36 at 3,
+    80 at 2) and sampled crest (1095 m at 4 deg, 1173 m at 2)."""
+    from water_simulator_b200 import globe
+    sim = S.sphere(swe.ShallowWater, globe.GLOBE_BEDS["seamount"]["bed"], deg)
+    sv = globe.surveyBed(sim)
+    assert sv["dry"] == dry
+    if crest is not None:
+        assert round(sv["crest"]) == crest
+    assert sv["max"] == sv["crest"] and sv["min"] < -3999
+    sim.close()
+
+
+def test_drop_bump_adds_to_wet_cells_only(swe):
+    from water_simulator_b200 import globe
+    sim = S.sphere(swe.ShallowWater, globe.GLOBE_BEDS["seamount"]["bed"], 4)
+    before = np.array(sim.field("h"))
+    globe.dropBump(sim, -40, 30, amp=2.0, sigmaDeg=10)
+    after = np.array(sim.field("h"))
+    for j in range(sim.ny):
+        for i in range(sim.nx):
+            k = sim.idx(i, j)
+            lo, la = sim.cellLonLat(i, j)
+            e = 2.0 * math.exp(-((globe.wrapLon(lo + 40) ** 2 + (la - 30) ** 2) / (2 * 10 * 10)))
+            if before[k] > sim.minDepth:
+                assert abs(after[k] - (before[k] + e)) <= 1e-12 * after[k]
+            else:
+                assert after[k] == before[k]
+    sim.step()                                  # the bumped state reaches the device
+    assert sim.volume() > 0
+    sim.close()

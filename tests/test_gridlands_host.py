@@ -1,10 +1,13 @@
-"""Host side of the gridlands import (src/gridlands.mjs): document checks that
-throw before anything is decoded, waterbodies / verifyInvariants /
-settleLakes on a synthetic export.  No GPU."""
+"""The gridlands import (src/gridlands.mjs): document checks that throw
+before anything is decoded (no GPU), and waterbodies / verifyInvariants /
+settleLakes on a synthetic export, whose bodies are labelled by the
+device's connected-components pass (GPU) and checked against a flood-fill
+oracle and the export's known lakes."""
 import numpy as np
 import pytest
 
 from gridlands_doc import make_doc, terrain_arrays
+from gridlands_oracle import flood_bodies
 
 
 def test_document_checks(swe):
@@ -30,6 +33,42 @@ def test_layer_checks_before_decoding(swe):
         gl.decodeF32({"encoding": "b64f16le", "data": ""}, 4, "bedM")
 
 
+def _same_bodies(got, want):
+    assert len(got) == len(want)
+    for g, w in zip(got, want):
+        assert g["level"] == w["level"] and g["spread"] == w["spread"]
+        assert g["ringMin"] == w["ringMin"] and g["perch"] == w["perch"] and g["isOcean"] == w["isOcean"]
+        assert list(g["cells"]) == w["cells"]
+
+
+@pytest.mark.gpu
+def test_device_bodies_match_the_flood_fill(swe):
+    """Random wet/dry maps with many bodies of every shape (spirals of one
+    cell, bodies touching the edges, one body over the whole grid)."""
+    from water_simulator_b200 import gridlands as gl
+    rng = np.random.default_rng(4)
+    for W, H, p in ((64, 48, 0.55), (200, 150, 0.6), (1, 37, 0.5), (41, 1, 0.5), (9, 7, 1.0), (128, 96, 0.45)):
+        bed = rng.uniform(-5, 5, (H, W)).astype(np.float32)
+        srf = np.where(rng.uniform(0, 1, (H, W)) < p, bed + rng.uniform(0.01, 2, (H, W)), bed).astype(np.float32)
+        _same_bodies(gl.waterbodies(bed, srf, W, H), flood_bodies(bed, srf, W, H))
+    # a one-cell-wide spiral: the longest chain a union-find can meet
+    W = H = 61
+    wet = np.zeros((H, W), bool)
+    r0, c0, r1, c1 = 0, 0, H - 1, W - 1
+    while r0 <= r1 and c0 <= c1:
+        wet[r0, c0:c1 + 1] = True
+        wet[r0:r1 + 1, c1] = True
+        wet[r1, c0:c1 + 1] = True
+        if c0 + 2 <= c1:
+            wet[r0 + 2:r1 + 1, c0] = True
+        r0, c0, r1, c1 = r0 + 2, c0 + 2, r1 - 2, c1 - 2
+    bed = np.zeros((H, W), np.float32)
+    srf = np.where(wet, 1.0, 0.0).astype(np.float32)
+    _same_bodies(gl.waterbodies(bed, srf, W, H), flood_bodies(bed, srf, W, H))
+    assert gl.waterbodies(np.zeros((3, 3), np.float32), np.zeros((3, 3), np.float32), 3, 3) == []
+
+
+@pytest.mark.gpu
 def test_waterbodies_and_invariants(swe):
     from water_simulator_b200 import gridlands as gl
     W, H = 64, 48
@@ -61,6 +100,7 @@ def test_waterbodies_and_invariants(swe):
     assert inv["wet"] == len(wet) and inv["cells"] == W * H
 
 
+@pytest.mark.gpu
 def test_settle_lowers_only_the_perched_lake(swe):
     from water_simulator_b200 import gridlands as gl
     W, H = 64, 48

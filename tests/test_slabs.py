@@ -293,3 +293,59 @@ def test_local_slabs_match_one_sphere_on_the_gpu():
             assert np.array_equal(run.gather(f).view(np.uint64), want.view(np.uint64)), (step, f)
     for sim in run.sims + [whole]:
         sim.close()
+
+
+def test_periodic_south_north_is_refused():
+    """A cut into row slabs cannot keep a periodic south / north boundary."""
+    sl = _slabs()
+
+    class Fake:
+        class _P:
+            name = "periodic"
+
+        class _R:
+            name = "reflect"
+        boundaries = {"west": _P, "east": _P, "south": _R, "north": _P}
+    slab = sl.Slab(NY, 0, 30)
+    with pytest.raises(ValueError, match="north boundary is periodic"):
+        sl.LocalSlabs([slab], [Fake()])
+    with pytest.raises(ValueError, match="north boundary is periodic"):
+        sl.check_cuttable(Fake())
+
+
+@pytest.mark.gpu
+def test_device_slabs_match_one_grid_on_the_gpu():
+    """The device data plane: three slab handles on one GPU exchange their
+    halos through device buffers on their own streams and step with the
+    minimum of their maxDt() taken on the device (no host round trip), bit
+    for bit like one handle of the whole grid.  The Flather side is a
+    device tide so nothing needs the host per step."""
+    sl = _slabs()
+    import __graft_entry__
+    swe = __graft_entry__.load_package()
+    b, eta = case()
+    tide = swe.Tide({"X": [0.1, 90.0]}, periods_hours={"X": 30.0 / 3600})
+
+    def make(ny, bb, ee):
+        sim = swe.ShallowWater(nx=NX, ny=ny, bed=bb, eta0=ee, **KW)
+        sim.boundaries = {"west": swe.flather(tide.signal()), "east": swe.reflect,
+                          "south": swe.reflect, "north": swe.reflect}
+        sim._prepare_flather()
+        return sim
+
+    whole = make(NY, b, eta)
+    slabs = [sl.Slab(NY, a, c) for a, c in sl.slab_rows(NY, 3)]
+    run = sl.LocalSlabs(slabs, [make(s.rows, s.take(b), s.take(eta)) for s in slabs], device=True)
+    for step in range(STEPS):
+        dt = run.step()
+        t0 = whole.t
+        assert whole.run(1) == 1
+        assert float(dt.item()) == whole.t - t0 or run.sims[0].t == whole.t
+        assert all(s.t == whole.t for s in run.sims)
+        for f in ("h", "hu", "hv"):
+            got = run.gather(f)
+            want = whole.get_rows(f, 2, NY).reshape(NY, -1)
+            assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), (step, f)
+    assert all(s.t == whole.t for s in run.sims)
+    for sim in run.sims + [whole]:
+        sim.close()

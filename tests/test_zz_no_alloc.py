@@ -54,6 +54,43 @@ def test_noalloc_max_dt_matches_handle_path(swe):
     sim.close()
 
 
+def test_noalloc_max_dt_all_dry_is_infinity(swe):
+    """No wet cell: maxDt() is Infinity (src/swe.mjs:646), on both paths."""
+    torch = pytest.importorskip("torch")
+    lib = swe.load_library()
+    sim = swe.ShallowWater(nx=40, ny=30, dx=2.0, bed=lambda x, y: 1.0, eta0=0.0)
+    assert sim.maxDt() == float("inf")
+    f = _device_copies(torch, sim)
+    out = torch.empty(1, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        out.fill_(-1.0)
+        assert _call(lib, torch, sim, f, out) == 0, lib.swe_last_error()
+        torch.cuda.synchronize()
+        assert out.item() == float("inf")
+    sim.close()
+
+
+def test_noalloc_max_dt_at_the_row_limit(swe):
+    """ny = SWE_NOALLOC_MAX_ROWS: every scratch slot is used, and the result
+    still equals the handle path's."""
+    torch = pytest.importorskip("torch")
+    lib = swe.load_library()
+    nx, ny = 8, 16384
+    rng = np.random.default_rng(3)
+    eta = 1.0 + 0.5 * rng.uniform(0, 1, (ny + 4, nx + 4))
+    sim = swe.ShallowWater(nx=nx, ny=ny, dx=1.5, bed=np.zeros((ny + 4, nx + 4)), eta0=eta)
+    sim.step()
+    want = sim.maxDt()
+    f = _device_copies(torch, sim)
+    out = torch.empty(1, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        out.fill_(-1.0)
+        assert _call(lib, torch, sim, f, out) == 0, lib.swe_last_error()
+        torch.cuda.synchronize()
+        assert out.item() == want
+    sim.close()
+
+
 def test_noalloc_max_dt_rejects_oversized_grid(swe):
     torch = pytest.importorskip("torch")
     lib = swe.load_library()

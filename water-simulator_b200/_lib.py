@@ -70,6 +70,10 @@ SIGNATURES = {
     "swe_set_field": [_P, _I, _DP],
     "swe_get_rows": [_P, _I, _I, _I, _DP],
     "swe_set_rows": [_P, _I, _I, _I, _DP],
+    "swe_get_rows_async": [_P, _I, _I, _I, _P],
+    "swe_set_rows_async": [_P, _I, _I, _I, _P],
+    "swe_max_dt_to": [_P, _P],
+    "swe_step_dt_from": [_P, _P],
     "swe_get_geom": [_P, _I, _DP],
     "swe_set_geom": [_P, _I, _DP],
     "swe_get_scalar": [_P, _I, _DP],
@@ -93,6 +97,8 @@ SIGNATURES = {
     "swe_energy": [_P, _DP],
     "swe_max_surface_deviation": [_P, _D, _DP],
     "swe_max_speed": [_P, _DP],
+    "swe_set_diag_order": [_P, _I],
+    "swe_eta_projection": [_P, _DP, _DP],
     "swe_finite": [_P, _IP],
     "swe_synchronize": [_P],
     "swe_get_stream": [_P, ctypes.POINTER(_P)],
@@ -104,6 +110,7 @@ SIGNATURES = {
     "swe_max_dt_noalloc": [_I, _I, _P, _P, _P, _P, _P, _D, _D, _P, _P],
     "swe_gridlands_decode": [ctypes.c_char_p, ctypes.c_size_t, _I, _P],
     "swe_gridlands_create": [ctypes.POINTER(SweOptions), ctypes.POINTER(SweGridlands), ctypes.POINTER(_P)],
+    "swe_gridlands_bodies": [_I, _I, _P, _P, _P],
     "swe_set_stage_kernels": [_P, _I],
     "swe_get_stage_kernels": [_P, _IP],
     "swe_render_map": [_P, _D, _D, _I, _P, _P],
@@ -121,6 +128,10 @@ SIGNATURES = {
     "swe_batch_autotune": [_P, _I, _IP, _DP],
     "swe_batch_run": [_P, _I],
     "swe_batch_synchronize": [_P],
+    "swe_batch_set_launch": [_P, _I],
+    "swe_batch_get_launch": [_P, _IP],
+    "swe_batch_set_wait_limit": [_P, _D],
+    "swe_batch_debug_hold": [_P, _I],
     "swe_batch_get_stream": [_P, ctypes.POINTER(_P)],
     "swe_batch_get_field": [_P, _I, _I, _DP],
     "swe_batch_get_scalar": [_P, _I, _I, _DP],

@@ -83,7 +83,27 @@ class Ensemble:
         check(self._lib.swe_batch_run(self._h, int(steps)))
 
     def synchronize(self):
+        """Wait for the ensemble; raises SweError (SWE_ETIMEOUT) when a
+        work-queue wait ran past its limit since the last call."""
         check(self._lib.swe_batch_synchronize(self._h))
+
+    @property
+    def launch(self):
+        """"queue": one persistent launch per step over a device work queue;
+        "phases": a launch per phase of the step."""
+        q = ctypes.c_int()
+        check(self._lib.swe_batch_get_launch(self._h, ctypes.byref(q)))
+        return "queue" if q.value else "phases"
+
+    def set_launch(self, launch):
+        check(self._lib.swe_batch_set_launch(self._h, {"phases": 0, "queue": 1}[launch]))
+
+    def set_wait_limit(self, seconds):
+        check(self._lib.swe_batch_set_wait_limit(self._h, float(seconds)))
+
+    def debug_hold(self, basin=-1):
+        """Test hook: never mark `basin`'s prepare done (-1: none)."""
+        check(self._lib.swe_batch_debug_hold(self._h, int(basin)))
 
     def field(self, basin, name):
         W, H = self.dims[basin]
@@ -122,11 +142,13 @@ class Ensemble:
                 d = json.load(f)
             if key in d:
                 self.set_schedule(**{k: d[key][k] for k in ("rows", "ctas", "order")})
+                self.set_launch(d[key].get("launch", "phases"))
                 return dict(d[key], cached=True)
         best = (ctypes.c_int * 4)()
         ms = ctypes.c_double()
         check(self._lib.swe_batch_autotune(self._h, int(trial_steps), best, ctypes.byref(ms)))
-        res = {"rows": best[0], "ctas": best[1], "order": best[2], "tiles": best[3], "ms_per_step": ms.value}
+        res = {"rows": best[0], "ctas": best[1], "order": best[2], "tiles": best[3], "ms_per_step": ms.value,
+               "launch": self.launch}
         if cache and key:
             d = {}
             if os.path.exists(cache):

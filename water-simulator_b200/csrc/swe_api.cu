@@ -74,6 +74,8 @@ struct swe_sim {
   double* d_geom = nullptr;
   double* d_part = nullptr;
   double* d_rows = nullptr;
+  double* d_coef = nullptr;                        // weights of swe_eta_projection (ny)
+  int diag_order = SWE_DIAG_REFERENCE;
   double* d_sponge = nullptr;
   swe::Control* d_ctl = nullptr;
   int bc[4];
@@ -280,9 +282,9 @@ swe::BCArgs bc_args(const swe_sim* s, double* const* f) {
   return a;
 }
 
-swe::PrepArgs prep_args(const swe_sim* s, int mode, double dt, double t_end) {
+swe::PrepArgs prep_args(const swe_sim* s, int mode, double dt, double t_end, const double* dt_dev = nullptr) {
   swe::PrepArgs p;
-  p.mode = mode; p.dt_host = dt; p.cfl = s->o.cfl; p.t_end = t_end;
+  p.mode = mode; p.dt_host = dt; p.cfl = s->o.cfl; p.t_end = t_end; p.dt_dev = dt_dev;
   for (int q = 0; q < 4; q++) { p.fl_kind[q] = s->fl_kind[q]; p.fl_eta[q] = s->fl_eta[q]; p.fl_u[q] = s->fl_u[q]; }
   return p;
 }
@@ -350,11 +352,11 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
   return SWE_OK;
 }
 
-int enqueue_step(swe_sim* s, int mode, double dt, double t_end) {
+int enqueue_step(swe_sim* s, int mode, double dt, double t_end, const double* dt_dev = nullptr) {
   // The tiled kernels, the ghost fills and prepare enter through pdl_enter,
   // so each may be scheduled while its predecessor drains.
   const bool pdl = s->pdl && s->stage_impl == 1;
-  CU(launch(pdl, swe::k_prepare, dim3(1), dim3(32), s->st, s->d_ctl, prep_args(s, mode, dt, t_end)));
+  CU(launch(pdl, swe::k_prepare, dim3(1), dim3(32), s->st, s->d_ctl, prep_args(s, mode, dt, t_end, dt_dev)));
   // Host-checked dt (mode 0) never reaches here refused.  In the device loop
   // a refused step (t reached t_end) changes nothing, ghosts included, as the
   // drivers' `while (sim.t < T)` loop stops calling step().
@@ -455,8 +457,8 @@ void free_all(swe_sim* s) {
   for (auto& g : s->graphs) if (g.exec) cudaGraphExecDestroy(g.exec);
   double** ptrs[] = {&s->d_b, &s->d_A[0], &s->d_A[1], &s->d_A[2], &s->d_B[0], &s->d_B[1], &s->d_B[2],
                      &s->d_h0[0], &s->d_h0[1], &s->d_h0[2], &s->d_res[0], &s->d_res[1], &s->d_res[2],
-                     &s->d_res[3], &s->d_nfield, &s->d_geom, &s->d_part, &s->d_rows, &s->d_sponge,
-                     &s->d_split};
+                     &s->d_res[3], &s->d_nfield, &s->d_geom, &s->d_part, &s->d_rows, &s->d_coef,
+                     &s->d_sponge, &s->d_split};
   for (double** p : ptrs) if (*p) { cudaFree(*p); *p = nullptr; }
   if (s->d_ctl) cudaFree(s->d_ctl);
   if (s->st) cudaStreamDestroy(s->st);
@@ -628,6 +630,52 @@ int swe_set_rows(swe_sim* s, int field, int row0, int nrows, const double* in) {
   CU(cudaMemcpyAsync(field_ptr(s, field) + off, in, nb, cudaMemcpyHostToDevice, s->st));
   if (field != SWE_FIELD_B && forget_dry(s)) return SWE_ECUDA;
   s->cfl_valid = false;
+  return SWE_OK;
+}
+
+static int rows_args(swe_sim* s, int field, int row0, int nrows, const void* p, const char* who) {
+  if (!s || !p) return fail(SWE_EINVAL, std::string(who) + ": null argument");
+  if (field != SWE_FIELD_B && field != SWE_FIELD_H && field != SWE_FIELD_HU && field != SWE_FIELD_HV)
+    return fail(SWE_EINVAL, std::string(who) + ": b, h, hu or hv");
+  if (row0 < 0 || nrows < 0 || row0 > s->H - nrows) return fail(SWE_EINVAL, std::string(who) + ": rows out of range");
+  return SWE_OK;
+}
+
+int swe_get_rows_async(swe_sim* s, int field, int row0, int nrows, double* dst) {
+  int rc = rows_args(s, field, row0, nrows, dst, "swe_get_rows_async");
+  if (rc || nrows == 0) return rc;
+  const size_t off = (size_t)row0 * s->W, nb = sizeof(double) * (size_t)nrows * s->W;
+  CU(cudaMemcpyAsync(dst, field_ptr(s, field) + off, nb, cudaMemcpyDefault, s->st));
+  return SWE_OK;
+}
+
+int swe_set_rows_async(swe_sim* s, int field, int row0, int nrows, const double* src) {
+  int rc = rows_args(s, field, row0, nrows, src, "swe_set_rows_async");
+  if (rc || nrows == 0) return rc;
+  const size_t off = (size_t)row0 * s->W, nb = sizeof(double) * (size_t)nrows * s->W;
+  CU(cudaMemcpyAsync(field_ptr(s, field) + off, src, nb, cudaMemcpyDefault, s->st));
+  if (field != SWE_FIELD_B && forget_dry(s)) return SWE_ECUDA;
+  s->cfl_valid = false;
+  return SWE_OK;
+}
+
+int swe_max_dt_to(swe_sim* s, double* dst) {
+  if (!s || !dst) return fail(SWE_EINVAL, "swe_max_dt_to: null argument");
+  int rc = ensure_cfl(s);
+  if (rc) return rc;
+  swe::k_dt_out<<<1, 32, 0, s->st>>>(s->d_ctl, s->o.cfl, dst);
+  CU(cudaGetLastError());
+  return SWE_OK;
+}
+
+int swe_step_dt_from(swe_sim* s, const double* dt) {
+  if (!s || !dt) return fail(SWE_EINVAL, "swe_step_dt_from: null argument");
+  int rc = sync_clock(s);
+  if (rc) return rc;
+  rc = enqueue_step(s, 4, 0, INFINITY, dt);
+  if (rc) return rc;
+  s->clock_valid = false;           // t and steps advanced on the device only
+  s->cfl_valid = true;
   return SWE_OK;
 }
 
@@ -836,7 +884,7 @@ int swe_apply_friction(swe_sim* s, double dt) {
 int swe_dry_clean(swe_sim* s, double* added) {
   if (!s) return fail(SWE_EINVAL, "null argument");
   swe::StageArgs a = stage_args(s, s->d_A, s->d_A);
-  swe::k_dry_clean<<<1, 1, 0, s->st>>>(a, s->d_ctl);
+  swe::k_dry_clean<<<1, swe::CHAIN_THREADS, 0, s->st>>>(a, s->d_ctl);
   CU(cudaGetLastError());
   if (forget_dry(s)) return SWE_ECUDA;
   swe::Control c;
@@ -957,26 +1005,46 @@ static int finish_diag(swe_sim* s, double* out) {
   return SWE_OK;
 }
 
+// Per-row sums (one warp per row) of `what`, then the rows in order.
+static int row_diag(swe_sim* s, int what, int mode, const double* w, double* out) {
+  swe::StageArgs a = stage_args(s, s->d_A, nullptr);
+  swe::k_row_sums<<<(s->ny + swe::ROWSUM_WARPS - 1) / swe::ROWSUM_WARPS, 32 * swe::ROWSUM_WARPS, 0, s->st>>>(
+      a, what, s->d_rows);
+  CU(cudaGetLastError());
+  swe::k_finish_sum<<<1, 1, 0, s->st>>>(s->d_rows, s->ny, mode, w, s->dx, s->dy, s->d_ctl);
+  CU(cudaGetLastError());
+  return finish_diag(s, out);
+}
+
 int swe_volume(swe_sim* s, double* out) {
   if (!s || !out) return fail(SWE_EINVAL, "null argument");
+  if (s->o.sphere) return row_diag(s, 0, 0, s->d_geom + SWE_GEOM_AREA * s->H + 2, out);
+  if (s->diag_order == SWE_DIAG_ROWS) return row_diag(s, 0, 1, nullptr, out);
   swe::StageArgs a = stage_args(s, s->d_A, nullptr);
-  if (s->o.sphere) {
-    swe::k_row_sums<<<(s->ny + 127) / 128, 128, 0, s->st>>>(a, 0, s->d_rows);
-    CU(cudaGetLastError());
-  }
-  swe::k_finish_sum<<<1, 1, 0, s->st>>>(a, 0, s->d_rows, s->d_geom + SWE_GEOM_AREA * s->H, s->dx, s->dy, s->d_ctl);
+  swe::k_volume_chain<<<1, swe::CHAIN_THREADS, 0, s->st>>>(a, s->dx, s->dy, s->d_ctl);
   CU(cudaGetLastError());
   return finish_diag(s, out);
 }
 
 int swe_energy(swe_sim* s, double* out) {
   if (!s || !out) return fail(SWE_EINVAL, "null argument");
-  swe::StageArgs a = stage_args(s, s->d_A, nullptr);
-  swe::k_row_sums<<<(s->ny + 127) / 128, 128, 0, s->st>>>(a, 1, s->d_rows);
-  CU(cudaGetLastError());
-  swe::k_finish_sum<<<1, 1, 0, s->st>>>(a, 1, s->d_rows, s->d_geom + SWE_GEOM_AREA * s->H, s->dx, s->dy, s->d_ctl);
-  CU(cudaGetLastError());
-  return finish_diag(s, out);
+  if (s->o.sphere) return row_diag(s, 1, 0, s->d_geom + SWE_GEOM_AREA * s->H + 2, out);
+  return row_diag(s, 1, 1, nullptr, out);
+}
+
+int swe_set_diag_order(swe_sim* s, int order) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (order != SWE_DIAG_REFERENCE && order != SWE_DIAG_ROWS)
+    return fail(SWE_EINVAL, "swe_set_diag_order: SWE_DIAG_REFERENCE or SWE_DIAG_ROWS");
+  s->diag_order = order;
+  return SWE_OK;
+}
+
+int swe_eta_projection(swe_sim* s, const double* coef, double* out) {
+  if (!s || !coef || !out) return fail(SWE_EINVAL, "null argument");
+  if (!s->d_coef) CU(cudaMalloc(&s->d_coef, sizeof(double) * std::max(1, s->ny)));
+  CU(cudaMemcpyAsync(s->d_coef, coef, sizeof(double) * s->ny, cudaMemcpyHostToDevice, s->st));
+  return row_diag(s, 2, 2, s->d_coef, out);
 }
 
 static int max_diag(swe_sim* s, int what, double ref, double* out) {

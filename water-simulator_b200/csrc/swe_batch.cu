@@ -96,9 +96,122 @@ k_batch_split_cells(BatchBasin* basins, const BatchTile* tiles, int ntiles) {
   }
 }
 
+// ---- one persistent launch per ensemble step --------------------------------
+// A device work queue holds every piece of one ensemble step, phase-major:
+//   phase 0  prepare          one item per basin   (dt, Flather values)
+//   phase 1  ghost fill of A  one item per basin
+//   phase 2  faces of A       one item per tile    (the tile list's order)
+//   phase 3  cells, stage 1   one item per tile    (the basin's last tile closes stage 1)
+//   phase 4  ghost fill of B  one item per basin
+//   phase 5  faces of B       one item per tile
+//   phase 6  cells, stage 2   one item per tile    (the basin's last tile closes the step)
+// Each CTA takes the next item from a queue head (one atomic) and, before it
+// touches memory, waits until the previous phase of the item's basin is
+// complete (a per-basin count: 1 or the basin's tile count).  Items are taken
+// in queue order, so every item a CTA waits on was taken earlier by a CTA
+// that is running; the waits therefore end, whatever the grid size.  Each
+// wait still carries a time limit: past it the CTA records a timeout, every
+// CTA drops the rest of the step, and the host reads SWE_ETIMEOUT.  The
+// completion count is released after a __threadfence and read back with one,
+// so a phase's writes are visible to the next phase's CTAs, as at a kernel
+// boundary.  The tile functions are the single-grid ones: each basin's result
+// is bit-identical to advancing it alone.
+constexpr int QPHASES = 7;
+
+struct QueueCtl {
+  int* head;                  // next item; reset before every launch
+  int* done;                  // [basin * QPHASES + phase]; reset before every launch
+  int* err;                   // 1: a wait ran out of time (sticky until the host reads it)
+  long long limit_ns;         // the time limit of one wait
+  int hold;                   // debug: a basin whose prepare is never marked done (-1: none)
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Thread 0: until done[slot] >= need, bounded by the time limit.
+__device__ bool queue_wait(const QueueCtl& q, int slot, int need) {
+  volatile int* d = q.done;
+  volatile int* e = q.err;
+  if (d[slot] >= need) return true;
+  const unsigned long long t0 = global_ns();
+  while (d[slot] < need) {
+    if (*e) return false;
+    if ((long long)(global_ns() - t0) > q.limit_ns) {
+      atomicExch(q.err, 1);
+      return false;
+    }
+    __nanosleep(256);
+  }
+  return true;
+}
+
+union QueueSmem {
+  swe::FacesSmem f;
+  swe::CellsSmem c;
+};
+
+#ifndef SWE_QUEUE_MIN_BLOCKS
+#define SWE_QUEUE_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(swe::SP_THREADS, SWE_QUEUE_MIN_BLOCKS)
+k_batch_queue_step(BatchBasin* basins, const BatchTile* tiles, int nb, int ntiles, QueueCtl q) {
+  __shared__ QueueSmem sm;
+  __shared__ int s_item, s_go;
+  const int total = 3 * nb + 4 * ntiles;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = *(volatile int*)q.err ? total : atomicAdd(q.head, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= total) return;                       // uniform
+    // the item's phase, basin and (tile phases) tile
+    int phase, j = it;
+    const int len[QPHASES] = {nb, nb, ntiles, ntiles, nb, ntiles, ntiles};
+    for (phase = 0; phase < QPHASES - 1 && j >= len[phase]; phase++) j -= len[phase];
+    const bool per_tile = phase == 2 || phase == 3 || phase == 5 || phase == 6;
+    const BatchTile tile = per_tile ? tiles[j] : BatchTile{j, 0, 0, 0, 0};
+    const int b = tile.basin;
+    const BatchBasin& B = basins[b];
+    if (threadIdx.x == 0) {
+      bool ok = true;
+      if (phase > 0) {
+        const int prev = phase - 1;
+        const int need = (prev == 2 || prev == 3 || prev == 5) ? B.s1.nblocks : 1;
+        ok = queue_wait(q, b * QPHASES + prev, need);
+      }
+      __threadfence();
+      s_go = ok ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_go) return;                             // timed out: drop the rest of the step
+    const bool stop = phase > 0 && B.ctl->stop != 0;  // set by this step's prepare
+    switch (phase) {
+      case 0: if (threadIdx.x == 0) swe::prepare_one(B.ctl, B.prep); break;
+      case 1: if (!stop) swe::apply_bc_range(B.bcA, B.ctl, threadIdx.x, blockDim.x); break;
+      case 2: if (!stop) swe::split_faces_tile(B.s1, B.sp, tile.strip, tile.y0, sm.f); break;
+      case 3: if (!stop) swe::split_cells_tile<1>(B.s1, B.sp, B.ctl, tile.strip, tile.y0, tile.part, B.s1.nblocks,
+                                                  sm.c, true);
+              break;
+      case 4: if (!stop) swe::apply_bc_range(B.bcB, B.ctl, threadIdx.x, blockDim.x); break;
+      case 5: if (!stop) swe::split_faces_tile(B.s2, B.sp, tile.strip, tile.y0, sm.f); break;
+      default: if (!stop) swe::split_cells_tile<2>(B.s2, B.sp, B.ctl, tile.strip, tile.y0, tile.part,
+                                                   B.s2.nblocks, sm.c, true);
+               break;
+    }
+    __syncthreads();                               // the item's writes, then its completion
+    if (threadIdx.x == 0 && !(phase == 0 && b == q.hold)) {
+      __threadfence();
+      atomicAdd(q.done + b * QPHASES + phase, 1);
+    }
+  }
+}
+
 int fail(int code, const std::string& m) { swe_host::set_error(m); return code; }
 
-#define CU(call)                                                                      \
+#define CU(call)                                                                   \
   do {                                                                                \
     cudaError_t e_ = (call);                                                          \
     if (e_ != cudaSuccess) return fail(SWE_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
@@ -126,6 +239,11 @@ struct swe_batch {
   cudaGraphExec_t gexec = nullptr;
   int g_steps = 0;
   unsigned long long version = 1, g_version = 0;
+  // one persistent launch per step over a work queue (tiled pair only)
+  int queue = 0;
+  int* d_queue = nullptr;           // head, done[nb * QPHASES], err
+  long long wait_ns = 2000000000LL; // a wait gives up after 2 s
+  int hold = -1;
 };
 
 namespace {
@@ -200,7 +318,31 @@ int build_tiles(swe_batch* s) {
   return SWE_OK;
 }
 
+int queue_grid(const swe_batch* s) {
+  if (s->ctas > 0) return s->ctas;
+  int dev = 0, sms = 148, occ = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_queue_step, swe::SP_THREADS, 0);
+  return sms * std::max(occ, 1);                 // one CTA per resident slot
+}
+
+int enqueue_queue_step(swe_batch* s) {
+  const size_t nint = 1 + (size_t)QPHASES * s->nb;   // head and the completion counts (not err)
+  CU(cudaMemsetAsync(s->d_queue, 0, sizeof(int) * nint, s->st));
+  QueueCtl q;
+  q.head = s->d_queue;
+  q.done = s->d_queue + 1;
+  q.err = s->d_queue + nint;
+  q.limit_ns = s->wait_ns;
+  q.hold = s->hold;
+  k_batch_queue_step<<<queue_grid(s), swe::SP_THREADS, 0, s->st>>>(s->d_basins, s->d_tiles, s->nb, s->ntiles, q);
+  CU(cudaGetLastError());
+  return SWE_OK;
+}
+
 int enqueue_batch_step(swe_batch* s) {
+  if (s->queue && s->impl == 1) return enqueue_queue_step(s);
   k_batch_prepare<<<(s->nb + 63) / 64, 64, 0, s->st>>>(s->d_basins, s->nb);
   CU(cudaGetLastError());
   int most = 0;
@@ -283,6 +425,7 @@ void free_batch(swe_batch* s) {
   if (s->ctls) cudaFree(s->ctls);
   if (s->d_basins) cudaFree(s->d_basins);
   if (s->d_tiles) cudaFree(s->d_tiles);
+  if (s->d_queue) cudaFree(s->d_queue);
   if (s->save) cudaFree(s->save);
   if (s->st) cudaStreamDestroy(s->st);
 }
@@ -332,7 +475,9 @@ int swe_batch_create(int n, const swe_options* opts, const double* const* b, con
       cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) ||
       cudaMalloc(&s->pool, sizeof(double) * total) ||
       cudaMalloc(&s->ctls, sizeof(Control) * n) ||
-      cudaMalloc(&s->d_basins, sizeof(BatchBasin) * n))
+      cudaMalloc(&s->d_basins, sizeof(BatchBasin) * n) ||
+      cudaMalloc(&s->d_queue, sizeof(int) * (2 + (size_t)QPHASES * n)) ||
+      cudaMemsetAsync(s->d_queue, 0, sizeof(int) * (2 + (size_t)QPHASES * n), s->st))
     return bail(fail(SWE_ECUDA, std::string("swe_batch_create: ") + cudaGetErrorString(cudaGetLastError())));
   cudaMemsetAsync(s->ctls, 0, sizeof(Control) * n, s->st);
   cudaMemsetAsync(s->pool, 0, sizeof(double) * total, s->st);
@@ -465,6 +610,43 @@ int swe_batch_run(swe_batch* s, int steps) {
 int swe_batch_synchronize(swe_batch* s) {
   if (!s) return fail(SWE_EINVAL, "null argument");
   CU(cudaStreamSynchronize(s->st));
+  int* err = s->d_queue + 1 + (size_t)QPHASES * s->nb;
+  int e = 0;
+  CU(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    CU(cudaMemset(err, 0, sizeof(int)));
+    return fail(SWE_ETIMEOUT, "swe_batch: a work-queue wait ran past its time limit; the steps in flight "
+                              "were dropped and the basins' state is not a completed step");
+  }
+  return SWE_OK;
+}
+
+int swe_batch_set_launch(swe_batch* s, int queue) {
+  if (!s || (queue != 0 && queue != 1)) return fail(SWE_EINVAL, "swe_batch_set_launch: 0 (a launch per phase) or 1");
+  if (queue && s->impl != 1)
+    return fail(SWE_EINVAL, "swe_batch_set_launch: the work queue runs the tiled stage pair (schedule rows 0)");
+  s->queue = queue;
+  s->version++;
+  return SWE_OK;
+}
+
+int swe_batch_get_launch(swe_batch* s, int* queue) {
+  if (!s || !queue) return fail(SWE_EINVAL, "null argument");
+  *queue = s->queue && s->impl == 1 ? 1 : 0;
+  return SWE_OK;
+}
+
+int swe_batch_set_wait_limit(swe_batch* s, double seconds) {
+  if (!s || !(seconds > 0) || !(seconds <= 60)) return fail(SWE_EINVAL, "swe_batch_set_wait_limit: 0 < seconds <= 60");
+  s->wait_ns = (long long)(seconds * 1e9);
+  s->version++;
+  return SWE_OK;
+}
+
+int swe_batch_debug_hold(swe_batch* s, int basin) {
+  if (!s || basin < -1 || basin >= s->nb) return fail(SWE_EINVAL, "swe_batch_debug_hold: a basin or -1");
+  s->hold = basin;
+  s->version++;
   return SWE_OK;
 }
 
@@ -531,18 +713,23 @@ int swe_batch_autotune(swe_batch* s, int trial_steps, int* best4, double* best_m
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_split, k_batch_split_faces<2>, swe::SP_THREADS, 0);
   const int rows_c[] = {0, 16, 24, 32, 48, 64};          // 0: the tiled pair
   double best = INFINITY;
-  int bi = s->impl, br = s->rows, bc = s->ctas, bo = s->order;
+  int bi = s->impl, br = s->rows, bc = s->ctas, bo = s->order, bq = s->queue;
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
+  // candidates: (rows, ctas index, order) with a launch per phase, then the
+  // tiled pair as one queue launch per step over a resident or a
+  // one-per-SM grid
   for (int r : rows_c)
-    for (int ci = 0; ci < 3; ci++)
+    for (int ci = 0; ci < 5; ci++)
       for (int o = 0; o < 3; o++) {
+        const bool queue = ci >= 3;
+        if (queue && r != 0) continue;
         const int per_sm = std::max(r == 0 ? occ_split : occ, 1);
-        const int c = ci == 0 ? 0 : ci * sms * per_sm;
+        const int c = queue ? (ci == 3 ? 0 : sms) : (ci == 0 ? 0 : ci * sms * per_sm);
         s->impl = r == 0 ? 1 : 0;
         if (r) s->rows = r;
-        s->ctas = c; s->order = o;
+        s->ctas = c; s->order = o; s->queue = queue ? 1 : 0;
         rc = build_tiles(s);
         if (rc) return rc;
         rc = run_steps(s, 1);                    // warm
@@ -554,13 +741,15 @@ int swe_batch_autotune(swe_batch* s, int trial_steps, int* best4, double* best_m
         CU(cudaEventSynchronize(e1));
         float ms = 0;
         CU(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) { best = ms; bi = s->impl; br = s->rows; bc = c; bo = o; }
+        if (ms < best) { best = ms; bi = s->impl; br = s->rows; bc = c; bo = o; bq = s->queue; }
         rc = snapshot(true);
+        if (rc) return rc;
+        rc = swe_batch_synchronize(s);           // a timed-out trial reports here
         if (rc) return rc;
       }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  s->impl = bi; s->rows = br; s->ctas = bc; s->order = bo;
+  s->impl = bi; s->rows = br; s->ctas = bc; s->order = bo; s->queue = bq;
   rc = build_tiles(s);
   if (rc) return rc;
   CU(cudaStreamSynchronize(s->st));

@@ -209,6 +209,75 @@ int decode_layer(const char* b64, size_t len, long long n, float* out, cudaStrea
   return SWE_OK;
 }
 
+// ---- connected waterbodies (src/gridlands.mjs:107-139) ----------------------
+// Wet cells (surface - bed > 0, in double) are grouped into 4-connected
+// bodies by a lock-free union-find over the grid: every wet cell unites
+// with its wet east and south neighbours.  A union always hangs the larger
+// root under the smaller, so parent[k] <= k holds throughout and every root
+// is its body's lowest cell index -- the cell the reference's row-major
+// scan starts that body's flood fill from.  find() walks strictly
+// decreasing indices, so it ends; a union retries only when another thread
+// has just hung its root (lock-free progress), and gives up after
+// CCL_TRIES attempts with an error flag rather than spin.
+constexpr int CCL_TRIES = 1 << 20;
+
+__device__ __forceinline__ bool ccl_wet(const float* bed, const float* srf, long long k) {
+  return (double)srf[k] - (double)bed[k] > 0;
+}
+
+__device__ __forceinline__ int ccl_find(int* parent, int x) {
+  volatile int* p = parent;
+  int up = p[x];
+  while (up != x) {
+    const int upup = p[up];
+    if (upup != up) p[x] = upup;                  // path halving: an ancestor, never a root's slot
+    x = up;
+    up = upup;
+  }
+  return x;
+}
+
+__global__ void k_ccl_init(const float* bed, const float* srf, long long n, int* parent) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    parent[k] = ccl_wet(bed, srf, k) ? (int)k : -1;
+}
+
+__global__ void k_ccl_merge(int W, int H, int* parent, int* bad) {
+  const long long n = (long long)W * H;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    if (parent[k] < 0) continue;
+    const int c = (int)(k % W), r = (int)(k / W);
+    for (int d = 0; d < 2; d++) {
+      const long long m = d == 0 ? k + 1 : k + W;
+      if ((d == 0 && c + 1 >= W) || (d == 1 && r + 1 >= H) || parent[m] < 0) continue;
+      int a = (int)k, b = (int)m;
+      bool done = false;
+      for (int it = 0; it < CCL_TRIES && !done; it++) {
+        a = ccl_find(parent, a);
+        b = ccl_find(parent, b);
+        if (a == b) { done = true; break; }
+        if (a > b) { const int t = a; a = b; b = t; }
+        const int old = atomicCAS(&parent[b], b, a);   // b still a root: hang it under a
+        if (old == b) done = true;
+        else b = old;                                 // b was just hung elsewhere
+      }
+      if (!done) atomicExch(bad, 1);
+    }
+  }
+}
+
+// After the merge the forest no longer changes: each wet cell's root, by a
+// walk that writes nothing (a shortcut written here could overwrite the
+// root another thread just stored).
+__global__ void k_ccl_flatten(long long n, const int* __restrict__ parent, int* __restrict__ label) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    int x = parent[k];
+    if (x >= 0)
+      while (parent[x] != x) x = parent[x];
+    label[k] = x;
+  }
+}
+
 int load_layer(const char* b64, size_t len, const float* host, long long n, float* out, cudaStream_t st,
                const char* name) {
   if (host) {
@@ -237,6 +306,38 @@ int swe_gridlands_decode(const char* b64, size_t len, int n, float* out) {
   }
   cudaStreamDestroy(st);
   return rc;
+}
+
+int swe_gridlands_bodies(int W, int H, const float* bed, const float* surface, int* label) {
+  if (W < 1 || H < 1 || !bed || !surface || !label)
+    return fail(SWE_EINVAL, "swe_gridlands_bodies: W, H >= 1 and non-null arrays");
+  const long long n = (long long)W * H;
+  if (n > 0x7fffffffLL) return fail(SWE_EINVAL, "swe_gridlands_bodies: more than 2^31 - 1 cells");
+  cudaStream_t st;
+  GL_CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); } } sg{st};
+  DevBuf layers, links, flag;
+  GL_CU(cudaMalloc(&layers.p, sizeof(float) * n * 2));
+  GL_CU(cudaMalloc(&links.p, sizeof(int) * n * 2));
+  GL_CU(cudaMalloc(&flag.p, sizeof(int)));
+  float* d_bed = static_cast<float*>(layers.p);
+  float* d_srf = d_bed + n;
+  int* parent = static_cast<int*>(links.p);
+  int* d_label = parent + n;
+  GL_CU(cudaMemcpyAsync(d_bed, bed, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  GL_CU(cudaMemcpyAsync(d_srf, surface, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  GL_CU(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+  const int nb = grid_blocks(n);
+  k_ccl_init<<<nb, 256, 0, st>>>(d_bed, d_srf, n, parent);
+  k_ccl_merge<<<nb, 256, 0, st>>>(W, H, parent, static_cast<int*>(flag.p));
+  k_ccl_flatten<<<nb, 256, 0, st>>>(n, parent, d_label);
+  GL_CU(cudaGetLastError());
+  int bad = 0;
+  GL_CU(cudaMemcpyAsync(&bad, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GL_CU(cudaMemcpyAsync(label, d_label, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  GL_CU(cudaStreamSynchronize(st));
+  if (bad) return fail(SWE_ETIMEOUT, "swe_gridlands_bodies: a union did not settle within its retry limit");
+  return SWE_OK;
 }
 
 int swe_gridlands_create(const swe_options* o, const swe_gridlands* g, swe_sim** out) {

@@ -109,10 +109,11 @@ struct StageArgs {
 
 // ---------------------------------------------------------------------------
 // prepare: dt of the next step (src/swe.mjs:783-784) and the Flather values.
-// mode 0: dt = dt_host; mode 1: dt = cfl/next_max (step()); mode 2: fixed dt
-// clamped to t_end - t; mode 3: min(maxDt, t_end - t).
+// mode 0: dt = dt_host (checked on the host); 1: cfl / next_max (step());
+// 2: a fixed dt clamped to t_end - t; 3: min(maxDt, t_end - t); 4: *dt_dev,
+// a dt another kernel or a collective left in device memory.
 struct PrepArgs {
-  int mode; double dt_host; double cfl; double t_end;
+  int mode; double dt_host; double cfl; double t_end; const double* dt_dev;
   int fl_kind[4];           // 0 host value, 1 tide table
   double fl_eta[4], fl_u[4];
 };
@@ -121,6 +122,7 @@ __device__ __forceinline__ void prepare_one(Control* ctl, const PrepArgs& a) {
   double dt;
   if (a.mode == 0) dt = a.dt_host;
   else if (a.mode == 2) dt = jmin(a.dt_host, a.t_end - ctl->t);
+  else if (a.mode == 4) dt = *a.dt_dev;
   else {
     const double inv = ctl->next_max;
     double md = inv > 0 ? a.cfl / inv : INFINITY;
@@ -158,6 +160,15 @@ __device__ __forceinline__ void pdl_enter() {
 __global__ void k_prepare(Control* ctl, PrepArgs a) {
   pdl_enter();
   if (threadIdx.x == 0) prepare_one(ctl, a);
+}
+
+// maxDt() of the current state (src/swe.mjs:632-647) into device memory, for
+// a caller that combines it on the device (a row slab's all-reduce).
+__global__ void k_dt_out(const Control* ctl, double cfl, double* out) {
+  if (threadIdx.x == 0) {
+    const double inv = ctl->next_max;
+    *out = inv > 0 ? cfl / inv : INFINITY;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -712,16 +723,74 @@ __global__ void k_cfl_rate(StageArgs a, Control* ctl, double* part) {
 
 // dryClean over the interior alone (src/swe.mjs:734-745); sequential order
 // for the floored sum, as the reference.
-__global__ void k_dry_clean(StageArgs a, Control* ctl) {
+// Interior cells in the reference's row-major order, CHAIN_CELLS at a time,
+// for the sums whose order is one running sum over every cell: the block
+// stages a chunk into shared memory (coalesced within each row) while its
+// first thread adds the previous chunk left to right.
+constexpr int CHAIN_THREADS = 256, CHAIN_CELLS = 4 * CHAIN_THREADS;
+__device__ __forceinline__ int chain_cell(const StageArgs& a, int q) {
+  const int j = q / a.nx;
+  return (j + 2) * a.W + (q - j * a.nx) + 2;
+}
+
+// dryClean() (src/swe.mjs:734-745): every cell's update in parallel; the
+// floored mass is the running sum of -h over the floored cells in row-major
+// order, which is the reference's sum (its other cells add nothing).  A
+// chunk with no floored cell costs the first thread nothing.
+__global__ void __launch_bounds__(CHAIN_THREADS) k_dry_clean(StageArgs a, Control* ctl) {
+  __shared__ double buf[CHAIN_CELLS];
+  const int n = a.nx * a.ny, t = threadIdx.x;
   double added = 0;
-  for (int j = 2; j < a.H - 2; j++)
-    for (int i = 2; i < a.W - 2; i++) {
-      const int k = j * a.W + i;
-      double h = a.oh[k];
-      if (h < 0) { added -= h; h = 0; a.oh[k] = 0; }
-      if (h <= a.minDepth) { a.ohu[k] = 0; a.ohv[k] = 0; }
+  for (int c0 = 0; c0 < n; c0 += CHAIN_CELLS) {
+    int mine = 0;
+    for (int r = 0; r < 4; r++) {
+      const int q = c0 + r * CHAIN_THREADS + t;
+      double add = 0;
+      if (q < n) {
+        const int k = chain_cell(a, q);
+        double h = a.oh[k];
+        if (h < 0) { add = -h; h = 0; a.oh[k] = 0; mine = 1; }
+        if (h <= a.minDepth) { a.ohu[k] = 0; a.ohv[k] = 0; }
+      }
+      buf[r * CHAIN_THREADS + t] = add;
     }
-  ctl->diag = added;
+    if (__syncthreads_or(mine) && t == 0) {
+      const int m = min(CHAIN_CELLS, n - c0);
+      for (int q = 0; q < m; q++)
+        if (buf[q] != 0) added += buf[q];
+    }
+    __syncthreads();
+  }
+  if (t == 0) ctl->diag = added;
+}
+
+// The Cartesian volume() (src/swe.mjs:818-827): one running sum of h over
+// every interior cell in row-major order, then one multiply by dx and dy.
+// The order is the reference's exactly; the chunks of the next iteration are
+// loaded by the whole block while the first thread adds.
+__global__ void __launch_bounds__(CHAIN_THREADS) k_volume_chain(StageArgs a, double dx, double dy, Control* ctl) {
+  __shared__ double buf[2][CHAIN_CELLS];
+  const int n = a.nx * a.ny, t = threadIdx.x;
+  const int chunks = (n + CHAIN_CELLS - 1) / CHAIN_CELLS;
+  auto stage = [&](int c) {
+    for (int r = 0; r < 4; r++) {
+      const int q = c * CHAIN_CELLS + r * CHAIN_THREADS + t;
+      buf[c & 1][r * CHAIN_THREADS + t] = q < n ? a.h[chain_cell(a, q)] : 0.0;
+    }
+  };
+  double v = 0;
+  if (chunks > 0) stage(0);
+  __syncthreads();
+  for (int c = 0; c < chunks; c++) {
+    if (c + 1 < chunks) stage(c + 1);
+    if (t == 0) {
+      const int m = min(CHAIN_CELLS, n - c * CHAIN_CELLS);
+      const double* b = buf[c & 1];
+      for (int q = 0; q < m; q++) v += b[q];
+    }
+    __syncthreads();
+  }
+  if (t == 0) ctl->diag = v * dx * dy;
 }
 
 // applyFriction alone (src/swe.mjs:659-704).
@@ -744,43 +813,60 @@ __global__ void k_friction(StageArgs a, double dt) {
   }
 }
 
-// Per-row partial sums for volume/energy in the reference's order.
-// what: 0 sum h, 1 energy row (src/swe.mjs:862-877).
-__global__ void k_row_sums(StageArgs a, int what, double* rows) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.ny) return;
-  const int W = a.W;
+// Per-row sums in the reference's order (each row left to right from +0),
+// one warp per row: the lanes load 32 consecutive cells of the row at a time
+// (coalesced) and form each cell's term, lane 0 adds the 32 terms in order.
+// what: 0 h (volume, src/swe.mjs:829-834), 1 the energy term
+// (:862-877), 2 b + h (the eta projection of src/globe.mjs:1414-1421).
+// A cell the energy skips (h <= 0) adds +0 here, which leaves a sum that
+// started at +0 unchanged bit for bit (it can never be -0).
+constexpr int ROWSUM_WARPS = 4;
+__global__ void __launch_bounds__(32 * ROWSUM_WARPS) k_row_sums(StageArgs a, int what, double* rows) {
+  __shared__ double buf[ROWSUM_WARPS][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int j = blockIdx.x * ROWSUM_WARPS + w;
+  if (j >= a.ny) return;                            // the whole warp
+  const size_t base = (size_t)(j + 2) * a.W + 2;
   double row = 0;
-  for (int i = 0; i < a.nx; i++) {
-    const int k = (j + 2) * W + (i + 2);
-    const double hk = a.h[k];
-    if (what == 0) { row += hk; continue; }
-    if (hk <= 0) continue;
-    const double den = vel_den(hk, a.eps4);
-    const double u = vel_num(a.hu[k], hk) / den, v = vel_num(a.hv[k], hk) / den;
-    row += 0.5 * hk * (u * u + v * v) + 0.5 * SWE_G * hk * (hk + 2 * a.b[k]);
+  for (int i0 = 0; i0 < a.nx; i0 += 32) {
+    const int i = i0 + lane;
+    double term = 0;
+    if (i < a.nx) {
+      const size_t k = base + i;
+      const double hk = a.h[k];
+      if (what == 0) term = hk;
+      else if (what == 2) term = a.b[k] + hk;
+      else if (!(hk <= 0)) {
+        const double den = vel_den(hk, a.eps4);
+        const double u = vel_num(a.hu[k], hk) / den, v = vel_num(a.hv[k], hk) / den;
+        term = 0.5 * hk * (u * u + v * v) + 0.5 * SWE_G * hk * (hk + 2 * a.b[k]);
+      }
+    }
+    buf[w][lane] = term;
+    __syncwarp();
+    if (lane == 0) {
+      const int m = min(32, a.nx - i0);
+      for (int q = 0; q < m; q++) row += buf[w][q];
+    }
+    __syncwarp();
   }
-  rows[j] = row;
+  if (lane == 0) rows[j] = row;
 }
 
-// volume (src/swe.mjs:819-836) and energy (:862-877) from row sums, in order.
-// Cartesian volume is one running sum over all cells, so it is summed here
-// cell by cell, not from the row sums.
-__global__ void k_finish_sum(StageArgs a, int what, const double* rows, const double* area,
-                             double dx, double dy, Control* ctl) {
+// The rows summed in order: mode 0 sum rows[j] * w[j] (the sphere's volume
+// and energy with w = area, src/swe.mjs:829-836, 875), mode 1 (sum rows) *
+// dx * dy (the Cartesian energy, :876; the Cartesian volume in the row
+// order), mode 2 sum w[j] * rows[j] with the caller's weights (the
+// projection).  One thread: ny terms.
+__global__ void k_finish_sum(const double* rows, int ny, int mode, const double* w, double dx, double dy,
+                             Control* ctl) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double v = 0;
-  if (what == 0 && !a.sph) {
-    for (int j = 0; j < a.ny; j++)
-      for (int i = 0; i < a.nx; i++) v += a.h[(j + 2) * a.W + (i + 2)];
-    ctl->diag = v * dx * dy;
-    return;
+  for (int j = 0; j < ny; j++) {
+    if (mode == 1) v += rows[j];
+    else v += rows[j] * w[j];
   }
-  for (int j = 0; j < a.ny; j++) {
-    if (a.sph) v += rows[j] * area[j + 2];
-    else v += rows[j];
-  }
-  ctl->diag = a.sph ? v : v * dx * dy;
+  ctl->diag = mode == 1 ? v * dx * dy : v;
 }
 
 // what: 0 maxSurfaceDeviation(ref) (src/swe.mjs:880-892), 1 maxSpeed (:895-907),

@@ -31,11 +31,13 @@ constexpr int MAX_DEVICES = 64;
 static __device__ __align__(256) double g_noalloc_scratch[MAX_ROWS + 1];
 
 // Device address of g_noalloc_scratch on each device.  In host code the
-// symbol is only a host-side stand-in, so the address is looked up once per
-// device, with that device current, and passed to the kernel.
+// symbol is only a host-side stand-in, so the address is looked up on the
+// first call on each device, with that device current, and passed to the
+// kernel.  Only a successful lookup is kept: a failed one is tried again on
+// the next call.  The address belongs to the device's context, so it goes
+// stale after cudaDeviceReset(); the entry point is not for use after one.
 double* g_addr[MAX_DEVICES] = {};
-std::once_flag g_once[MAX_DEVICES];
-cudaError_t g_addr_err[MAX_DEVICES] = {};
+std::mutex g_addr_mu;
 
 // Each block reduces one interior row; the last block to finish reduces the
 // row maxima and writes dt = cfl / max (Infinity when no cell is wet),
@@ -102,16 +104,21 @@ extern "C" int swe_max_dt_noalloc(int nx, int ny, const double* h, const double*
     return SWE_ECUDA;
   }
   // Set-up on the first call on this device (before any stream capture).
-  std::call_once(g_once[dev], [dev] {
-    void* p = nullptr;
-    g_addr_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    g_addr[dev] = static_cast<double*>(p);
-  });
-  if (g_addr_err[dev] != cudaSuccess || !g_addr[dev]) {
-    swe_host::set_error(std::string("swe_max_dt_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(g_addr_err[dev]));
-    return SWE_ECUDA;
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_addr_mu);
+    if (!g_addr[dev]) {
+      void* p = nullptr;
+      const cudaError_t le = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (le != cudaSuccess || !p) {
+        swe_host::set_error(std::string("swe_max_dt_noalloc: cudaGetSymbolAddress failed: ") +
+                            cudaGetErrorString(le));
+        return SWE_ECUDA;
+      }
+      g_addr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_addr[dev];
   }
-  double* scratch = g_addr[dev];
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // The ticket must start at zero; clear it rather than trust the last call.
   e = cudaMemsetAsync(scratch, 0, sizeof(double), st);

@@ -8,8 +8,9 @@ clamped) and `eta0(x, y)` (nearest) sampling functions, the decoded arrays
 and the provenance.  Handing `t.bed` and `t.eta0` to `ShallowWater` builds
 the fields on the device from the layers (swe_gridlands_create) instead of
 calling the functions cell by cell; the values are the same doubles.
-`waterbodies`, `verifyInvariants` and `settleLakes` are the host-side checks
-and the opt-in repair of src/gridlands.mjs:108-220.
+`waterbodies` labels the wet bodies with a connected-components pass on the
+device (swe_gridlands_bodies); `verifyInvariants` and the opt-in
+`settleLakes` repair build on it (src/gridlands.mjs:107-220).
 """
 import ctypes
 import math
@@ -48,95 +49,103 @@ def decodeF32(layer, n, name):
     return out
 
 
+def body_labels(bedM, surfaceM, W, H):
+    """Each cell's waterbody, from the device's connected-components pass
+    (swe_gridlands_bodies): the lowest cell index of the cell's 4-connected
+    wet body (surface - bed > 0), -1 for a dry cell."""
+    bed = np.ascontiguousarray(bedM, dtype=np.float32).reshape(-1)
+    srf = np.ascontiguousarray(surfaceM, dtype=np.float32).reshape(-1)
+    n = int(W) * int(H)
+    if bed.size != n or srf.size != n:
+        raise ValueError(f"gridlands: layers of {bed.size} and {srf.size} cells for a {W}x{H} grid")
+    label = np.empty(n, dtype=np.int32)
+    check(_lib.load().swe_gridlands_bodies(int(W), int(H), bed.ctypes.data, srf.ctypes.data, label.ctypes.data))
+    return label
+
+
 def waterbodies(bedM, surfaceM, W, H):
-    """src/gridlands.mjs:108-139: 4-connected wet bodies with the lowest bed on
-    each one's boundary ring (its spill level)."""
-    bed = np.asarray(bedM).tolist()
-    srf = np.asarray(surfaceM).tolist()
-    n = W * H
-    seen = bytearray(n)
-    out = []
-    for k0 in range(n):
-        if seen[k0] or not (srf[k0] - bed[k0] > 0):
-            continue
-        level = srf[k0]
-        cells, ring, spread = [], set(), 0.0
-        stack = [k0]
-        seen[k0] = 1
-        while stack:
-            k = stack.pop()
-            cells.append(k)
-            if srf[k] != level:
-                spread = max(spread, abs(srf[k] - level))
-            c = k % W
-            r = (k - c) // W
-            nb = []
-            if c > 0:
-                nb.append(k - 1)
-            if c < W - 1:
-                nb.append(k + 1)
-            if r > 0:
-                nb.append(k - W)
-            if r < H - 1:
-                nb.append(k + W)
-            for m in nb:
-                if srf[m] - bed[m] > 0:
-                    if not seen[m]:
-                        seen[m] = 1
-                        stack.append(m)
-                else:
-                    ring.add(m)
-        ringMin = math.inf
-        for m in ring:
-            ringMin = min(ringMin, bed[m])
-        out.append({"level": level, "cells": cells, "spread": spread, "ringMin": ringMin,
-                    "perch": level - ringMin, "isOcean": level == 0})
-    return out
+    """The connected wet bodies with the lowest bed on each one's boundary
+    ring, its spill level (src/gridlands.mjs:107-139).
+
+    The bodies come from the device pass and are listed by their lowest cell
+    (the reference's scan order), each with its surface level at that cell,
+    its cells (ascending), the largest departure of its surface from that
+    level (spread), the lowest bed among the dry cells that touch it
+    (ringMin, Infinity if none), perch = level - ringMin and isOcean
+    (level 0).  The per-body reductions run over whole arrays at once."""
+    bed = np.asarray(bedM, dtype=np.float32).reshape(-1).astype(np.float64)
+    srf = np.asarray(surfaceM, dtype=np.float32).reshape(-1).astype(np.float64)
+    W, H = int(W), int(H)
+    label = body_labels(bedM, surfaceM, W, H)
+    wet = label >= 0
+    roots = np.flatnonzero(wet & (label == np.arange(label.size)))      # ascending = scan order
+    if roots.size == 0:
+        return []
+    body = np.full(label.size, -1, dtype=np.int64)                     # cell -> body number
+    index = np.full(label.size, -1, dtype=np.int64)
+    index[roots] = np.arange(roots.size)
+    body[wet] = index[label[wet]]
+    level = srf[roots]
+    spread = np.zeros(roots.size)
+    np.maximum.at(spread, body[wet], np.abs(srf[wet] - level[body[wet]]))
+    # the ring: dry 4-neighbours of a body's cells, each pair seen from the wet side
+    ring = np.full(roots.size, np.inf)
+    grid = np.arange(label.size).reshape(H, W)
+    for a, b in ((grid[:, :-1], grid[:, 1:]), (grid[:-1, :], grid[1:, :])):
+        a, b = a.reshape(-1), b.reshape(-1)
+        for inner, outer in ((a, b), (b, a)):
+            edge = wet[inner] & ~wet[outer]
+            np.minimum.at(ring, body[inner[edge]], bed[outer[edge]])
+    order = np.argsort(body[wet], kind="stable")
+    cells = np.split(np.flatnonzero(wet)[order], np.cumsum(np.bincount(body[wet], minlength=roots.size))[:-1])
+    return [{"level": float(level[q]), "cells": cells[q], "spread": float(spread[q]), "ringMin": float(ring[q]),
+             "perch": float(level[q] - ring[q]), "isOcean": bool(level[q] == 0)} for q in range(roots.size)]
 
 
 def verifyInvariants(t):
-    """src/gridlands.mjs:157-195: the exporter's guarantees re-derived from the
-    decoded arrays, plus the one the solver needs (no lake above its spill)."""
+    """The exporter's guarantees re-derived from the decoded arrays, and the
+    one the solver needs besides: no lake above its spill level
+    (src/gridlands.mjs:141-195).  A report; nothing is raised."""
     bedM, surfaceM, W, H = t.bedM, t.surfaceM, t.W, t.H
-    d = surfaceM.astype(np.float64) - bedM.astype(np.float64)
-    below = int(np.count_nonzero(d < 0))
-    worstBelow = float(min(0.0, d.min())) if d.size else 0.0
-    wet = int(np.count_nonzero(d > 0))
-    oceanCells = int(np.count_nonzero((surfaceM == 0) & (bedM < 0)))
+    b = np.asarray(bedM, dtype=np.float64).reshape(-1)
+    s = np.asarray(surfaceM, dtype=np.float64).reshape(-1)
+    d = s - b
     bodies = waterbodies(bedM, surfaceM, W, H)
-    lakes = [b for b in bodies if not b["isOcean"]]
-    notFlat = [b for b in bodies if b["spread"] > 0]
-    perched = sorted([b for b in lakes if b["perch"] > 1e-6], key=lambda b: -b["perch"])
-    perchedVolume = 0.0
-    for b in perched:
-        perchedVolume += len(b["cells"]) * b["perch"]
-    ocean = [b["perch"] for b in bodies if b["isOcean"]]
+    lakes = [x for x in bodies if not x["isOcean"]]
+    uneven = [x["spread"] for x in bodies if x["spread"] > 0]
+    perched = sorted((x for x in lakes if x["perch"] > 1e-6), key=lambda x: -x["perch"])
+    volume = 0.0
+    for x in perched:                            # summed in the report's order
+        volume += len(x["cells"]) * x["perch"]
+    sizes = [len(x["cells"]) for x in bodies]
+    ocean = [x["perch"] for x in bodies if x["isOcean"]]
     return {
-        "cells": W * H, "wet": wet, "oceanCells": oceanCells,
-        "surfaceBelowBed": below, "worstBelowBed": worstBelow, "dryMismatch": 0,
-        "bodies": len(bodies), "lakeBodies": len(lakes), "lakesNotFlat": len(notFlat),
-        "worstLakeSpread": max([b["spread"] for b in notFlat], default=0),
-        "largestBody": max([len(b["cells"]) for b in bodies], default=0),
+        "cells": int(W) * int(H), "wet": int(np.count_nonzero(d > 0)),
+        "oceanCells": int(np.count_nonzero((s == 0) & (b < 0))),
+        "surfaceBelowBed": int(np.count_nonzero(d < 0)), "worstBelowBed": float(min(0.0, d.min(initial=0.0))),
+        "dryMismatch": 0,
+        "bodies": len(bodies), "lakeBodies": len(lakes), "lakesNotFlat": len(uneven),
+        "worstLakeSpread": max(uneven, default=0), "largestBody": max(sizes, default=0),
         "perchedLakes": len(perched), "worstPerch": perched[0]["perch"] if perched else 0,
-        "perchedCells": sum(len(b["cells"]) for b in perched),
-        "perchedVolumeCells": perchedVolume,
+        "perchedCells": sum(len(x["cells"]) for x in perched), "perchedVolumeCells": volume,
         "worstOceanPerch": max(ocean, default=-math.inf),
     }
 
 
 def settleLakes(bedM, surfaceM, W, H):
-    """src/gridlands.mjs:209-219: lower every perched body to its spill level,
-    in place (float32, as the reference's Float32Array), and report it."""
-    bodies = waterbodies(bedM, surfaceM, W, H)
+    """Lower every perched body to its spill level in place (cells left above
+    it become dry) and report what moved (src/gridlands.mjs:197-220).  Opt-in:
+    a repair on this side, never applied unasked."""
     moved = []
-    for b in bodies:
-        if not (b["perch"] > 1e-6):
+    flat = surfaceM.reshape(-1)
+    bed = np.asarray(bedM).reshape(-1)
+    for x in waterbodies(bedM, surfaceM, W, H):
+        if not (x["perch"] > 1e-6):
             continue
-        to = b["ringMin"]
-        for k in b["cells"]:
-            surfaceM[k] = max(float(bedM[k]), to)
-        moved.append({"from": b["level"], "to": to, "drop": b["perch"], "cells": len(b["cells"])})
-    return {"bodiesMoved": len(moved), "worstDrop": max([m["drop"] for m in moved], default=0), "moved": moved}
+        k = x["cells"]
+        flat[k] = np.maximum(bed[k].astype(np.float64), x["ringMin"])
+        moved.append({"from": x["level"], "to": x["ringMin"], "drop": x["perch"], "cells": len(k)})
+    return {"bodiesMoved": len(moved), "worstDrop": max((m["drop"] for m in moved), default=0), "moved": moved}
 
 
 class GridlandsTerrain:

@@ -6,12 +6,13 @@ assignment is longest-processing-time first (largest basin onto the least
 loaded rank, ties to the lower rank), computed identically on every rank
 from the basin sizes alone.  The only collectives are the timing ones:
 a barrier around the timed region and the maximum of the ranks' times.
+
+torch.distributed carries those collectives; it is imported only by the
+functions that need a process group, so the assignment itself (and the
+rest of the package) imports without torch.
 """
 import datetime
 import os
-
-import torch
-import torch.distributed as dist
 
 
 def assign_basins(cells, world):
@@ -38,6 +39,11 @@ def rank_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def _dist():
+    import torch.distributed as dist
+    return dist
+
+
 def init_ranks(backend, device=None, timeout_s=120):
     """The process group for a multi-rank run (nothing for one rank).  The
     rendezvous address comes from MASTER_ADDR / MASTER_PORT; the short
@@ -48,19 +54,26 @@ def init_ranks(backend, device=None, timeout_s=120):
     kw = {"timeout": datetime.timedelta(seconds=timeout_s)}
     if device is not None:
         kw["device_id"] = device
-    dist.init_process_group(backend, **kw)
+    _dist().init_process_group(backend, **kw)
     return True
+
+
+def _active():
+    dist = _dist()
+    return dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1
 
 
 def max_over_ranks(value, device=None):
     """The largest of the ranks' values (the job's time is its slowest rank)."""
-    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+    if not _active():
         return float(value)
+    import torch
+    dist = _dist()
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
 
 def barrier():
-    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
-        dist.barrier()
+    if _active():
+        _dist().barrier()
