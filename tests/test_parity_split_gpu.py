@@ -96,3 +96,29 @@ def test_dry_tile_flags_follow_host_writes(swe, monkeypatch):
     for a, b in zip(fused[:3], split[:3]):
         assert np.array_equal(a, b)
     assert fused[3] == split[3]
+
+
+@pytest.mark.parametrize("nx,ny", [(256, 96), (255, 97), (30, 9)])
+def test_tensor_map_tile_copies_give_the_same_bits(swe, monkeypatch, nx, ny):
+    """The face kernel's state tile fetched by tensor-map copies (even padded
+    width) against the per-element copies (SWE_B200_TMA=0): the same bits
+    after 150 steps of a flooding beach with friction, tiles at every edge of
+    the grid included (the copies fill outside the grid with zeros).  An odd
+    padded width always takes the per-element copies."""
+    import numpy as np
+    from water_simulator_b200 import workloads
+
+    def run(tma):
+        monkeypatch.setenv("SWE_B200_TMA", "1" if tma else "0")
+        b, h = workloads.beach_dam_break(nx=nx, ny=ny, dx=8.0 * 256 / nx)
+        sim = swe.ShallowWater(nx=nx, ny=ny, dx=8.0 * 256 / nx, bed=b, eta0=b + h, manning=0.03)
+        sim.boundaries = {"west": swe.flather(swe.Tide({}, msl=0.0).signal()), "north": swe.outflow}
+        assert sim.run(150) == 150
+        out = [sim.field(f).view(np.uint64).copy() for f in ("h", "hu", "hv")] + [sim.t]
+        sim.close()
+        return out
+
+    a, b = run(True), run(False)
+    for x, y in zip(a[:3], b[:3]):
+        assert np.array_equal(x, y)
+    assert a[3] == b[3]

@@ -8,6 +8,7 @@
 #include "swe_split.cuh"
 
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>        // PFN_cuTensorMapEncodeTiled (fetched through the runtime, no -lcuda)
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -96,6 +97,8 @@ struct swe_sim {
   int pdl = 1;                                     // programmatic dependent launch in the stepping loop
   double* d_split = nullptr;
   int* d_odry[2] = {nullptr, nullptr};             // per tile of A / B: all h == 0 (swe_split.cuh)
+  swe::TileMaps tmaps[2];                          // the face kernel's tensor maps over A and B
+  int tma = 0;                                     // 1: they are in use
   swe::SplitBufs sb;
   dim3 sgrid;
   // Whether the tiled cell kernels may settle dry tiles (swe_split.cuh).
@@ -314,6 +317,40 @@ int launch_bc(swe_sim* s, double* const* f, int respect_stop, bool pdl = false) 
   return SWE_OK;
 }
 
+// Tensor maps of the face kernel's state tile (swe_split.cuh, TileMaps):
+// b, h, hu, hv of A (stage 1's input) and of B (stage 2's), each a 2-D
+// W x H array of doubles, box SSXT x SSY, zeros outside.  A row stride that
+// is not a multiple of 16 bytes (odd W), a driver without the encoder, or
+// SWE_B200_TMA=0 leaves the per-element copies in use (the same bits).
+void make_tile_maps(swe_sim* s) {
+  s->tma = 0;
+  const char* env = std::getenv("SWE_B200_TMA");
+  if (env && std::strcmp(env, "0") == 0) return;
+  if ((sizeof(double) * (size_t)s->W) % 16 != 0) return;
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)s->W, (cuuint64_t)s->H};
+  const cuuint64_t strides[1] = {(cuuint64_t)s->W * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)swe::SSXT, (cuuint32_t)swe::SSY};
+  const cuuint32_t estr[2] = {1, 1};
+  double* src[2][4] = {{s->d_b, s->d_A[0], s->d_A[1], s->d_A[2]}, {s->d_b, s->d_B[0], s->d_B[1], s->d_B[2]}};
+  for (int st = 0; st < 2; st++)
+    for (int f = 0; f < 4; f++) {
+      const CUresult r = encode(&s->tmaps[st].m[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, src[st][f], dims, strides,
+                                box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return;
+    }
+  s->tma = 1;
+}
+
 // One SSP-RK2 step on the device; `mode`/`dt`/`t_end` as k_prepare.
 // Buffers of the tiled stage kernels (faces and source terms).
 int ensure_split(swe_sim* s) {
@@ -341,7 +378,8 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
     sb.odry_in = s->d_odry[MODE == 1 ? 0 : 1];
     sb.odry_out = s->d_odry[MODE == 1 ? 1 : 0];
     const dim3 blk(swe::SP_THREADS);
-    CU(launch(pdl, swe::k_split_faces, s->sgrid, blk, s->st, a, sb, s->d_ctl));
+    if (s->tma) CU(launch(pdl, swe::k_split_faces_tma, s->sgrid, blk, s->st, a, sb, s->d_ctl, s->tmaps[MODE - 1]));
+    else CU(launch(pdl, swe::k_split_faces, s->sgrid, blk, s->st, a, sb, s->d_ctl));
     if (s->settle) CU(launch(pdl, swe::k_split_cells<MODE, true>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
     else CU(launch(pdl, swe::k_split_cells<MODE, false>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
     CU(launch(pdl, swe::k_split_close<MODE>, dim3(1), blk, s->st, a, s->d_ctl, (int)(s->sgrid.x * s->sgrid.y)));
@@ -553,6 +591,7 @@ int swe_create(const swe_options* o, const double* b, const double* h, swe_sim**
   else CUB(cudaMemsetAsync(s->d_b, 0, nb, s->st));
   if (h) CUB(cudaMemcpyAsync(s->d_A[0], h, nb, cudaMemcpyHostToDevice, s->st));
   if (upload_geom(s)) return bail(SWE_ECUDA);
+  make_tile_maps(s);
   {
     const char* env = std::getenv("SWE_B200_STAGE");
     s->stage_impl = (env && std::strcmp(env, "fused") == 0) ? 0 : (env && std::strcmp(env, "split") == 0) ? 1

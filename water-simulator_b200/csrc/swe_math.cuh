@@ -33,7 +33,16 @@ __host__ __device__ __forceinline__ double jmax0(double x) { return x > 0 ? x : 
 // Limiters, src/swe.mjs:88-141.  lim: 0 mc (default), 1 minmod, 2 central.
 __device__ __forceinline__ double limiter(int lim, double a, double b) {
   if (lim == 0) {                                   // mc, src/swe.mjs:133-138
-    if (a * b <= 0) return 0;
+    const double p = a * b;
+    if (p > 0) {
+      // a, b are then non-NaN and nonzero of one sign, so c is too and the
+      // three candidates are non-NaN and > +0: IEEE minNum is Math.min here.
+      const double c = 0.5 * (a + b);
+      const double m = fmin(fmin(fabs(c), 2 * fabs(a)), 2 * fabs(b));
+      return a > 0 ? m : -m;
+    }
+    if (p <= 0) return 0;
+    // a * b is NaN: Math.min's NaN rule decides
     const double c = 0.5 * (a + b);
     const double m = jmin(jmin(fabs(c), 2 * fabs(a)), 2 * fabs(b));
     return a > 0 ? m : -m;
@@ -50,7 +59,10 @@ __device__ __forceinline__ double limiter(int lim, double a, double b) {
 // h only, so callers that need u and v of one cell share it (same double).
 __device__ __forceinline__ double vel_den(double h, double eps4) {
   const double h4 = h * h * h * h;
-  return sqrt(h4 + jmax(h4, eps4));
+  // h4 is +0, positive or NaN; for a NaN h4 the sum is NaN whichever maximum
+  // is taken, so IEEE maxNum gives Math.max's result unless eps4 itself is
+  // NaN (a NaN minDepth), where Math.max is NaN.
+  return sqrt(h4 + (eps4 == eps4 ? fmax(h4, eps4) : eps4));
 }
 __device__ __forceinline__ double vel_num(double hq, double h) { return SWE_SQRT2 * h * hq; }
 __device__ __forceinline__ double vel(double hq, double h, double eps4) {

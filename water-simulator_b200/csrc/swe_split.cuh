@@ -37,6 +37,8 @@
 // for bit; only the memory traffic of dry land goes.
 #pragma once
 
+#include <cuda.h>                 // CUtensorMap
+
 #include "swe_kernels.cuh"
 
 namespace swe {
@@ -110,8 +112,17 @@ __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// The state tile is stored SSXT = SSX + 1 columns wide starting one column
+// further west (gi = i0 - 2 at column 0, so column TCOL + lx holds gi =
+// i0 - 1 + lx): that is the box a tensor-map copy can fetch, whose first
+// column must sit on a 16-byte boundary of the row (an even column index).
+// Each array starts on a 128-byte boundary for the same copy.
+constexpr int TCOL = 1, SSXT = SSX + TCOL;
 struct FacesSmem {
-  double b[SSY][SSX], h[SSY][SSX], U[SSY][SSX], V[SSY][SSX];
+  alignas(128) double b[SSY][SSXT];
+  alignas(128) double h[SSY][SSXT];
+  alignas(128) double U[SSY][SSXT];
+  alignas(128) double V[SSY][SSXT];
   double xs[4][SPY][SPX + 1];                   // x slopes of cols i0 .. i0+SPX, rows j0 .. j0+SPY-1
   double ys[4][SPY + 1][SPX];                   // y slopes of cols i0 .. i0+SPX-1, rows j0 .. j0+SPY
 };
@@ -122,7 +133,7 @@ __device__ __forceinline__ void split_faces_cell(const StageArgs& a, const Split
   const int W = a.W, H = a.H;
   const double dry = a.minDepth;
   const int k = gj * W + gi;
-  const int cx = lx + 1, cy = ly + 1;
+  const int cx = lx + 1 + TCOL, cy = ly + 1;
   const double bk = sm.b[cy][cx], hk = sm.h[cy][cx], Uk = sm.U[cy][cx], Vk = sm.V[cy][cx];
   const double xsE = sm.xs[0][ly][lx], xsB = sm.xs[1][ly][lx];
   const double nsE = sm.ys[0][ly][lx], nsB = sm.ys[1][ly][lx];
@@ -170,54 +181,70 @@ __device__ __forceinline__ void split_faces_cell(const StageArgs& a, const Split
   s.fy[F_M][k] = fy.M; s.fy[F_T][k] = fy.T; s.fy[F_NPL][k] = fy.N + fy.pL; s.fy[F_NPR][k] = fy.N + fy.pR;
 }
 
+__device__ __forceinline__ void split_faces_finish(const StageArgs& a, const SplitBufs& s, int tx, int ty,
+                                                   FacesSmem& sm, int t);
+
+// A tile whose 3 x 3 neighbourhood of tiles holds only h == 0 (outside the
+// grid counts as zero state) is dry with its halo: nothing to load.  Marks
+// it dry and returns true (uniform across the CTA).
+__device__ __forceinline__ bool split_faces_settled(const SplitBufs& s, int tx, int ty, int t) {
+  if (!(s.odry_in && s.dry && !s.sl[0])) return false;
+  int f = 1;
+  if (t < 9) {
+    const int r = t / 3, c = t - 3 * r, txn = tx - 1 + c, tyn = ty - 1 + r;
+    if (txn >= 0 && txn < s.ntx && tyn >= 0 && tyn < s.nty) f = s.odry_in[tyn * s.ntx + txn];
+  }
+  if (__syncthreads_and(f)) {
+    if (t == 0) s.dry[ty * s.ntx + tx] = 1;
+    return true;
+  }
+  return false;
+}
+
 // Faces and source terms of the tile (tx, ty).  Every thread of the CTA
 // calls it; it returns with the shared memory free for the next tile.
 __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const SplitBufs& s, int tx, int ty,
                                                  FacesSmem& sm) {
   const int W = a.W, H = a.H;
   const int i0 = tx * SPX, j0 = ty * SPY;
-  const double dry = a.minDepth, eps4 = a.eps4;
-  const bool order2 = a.order >= 2;
-  const bool sph = a.sph != 0;
-  const bool bedOn = order2 || sph;
   const int t = threadIdx.x;
-
-  // A tile whose 3 x 3 neighbourhood of tiles holds only h == 0 (outside
-  // the grid counts as zero state) is dry with its halo: nothing to load.
-  if (s.odry_in && s.dry && !s.sl[0]) {
-    int f = 1;
-    if (t < 9) {
-      const int r = t / 3, c = t - 3 * r, txn = tx - 1 + c, tyn = ty - 1 + r;
-      if (txn >= 0 && txn < s.ntx && tyn >= 0 && tyn < s.nty) f = s.odry_in[tyn * s.ntx + txn];
-    }
-    if (__syncthreads_and(f)) {                   // uniform across the CTA
-      if (t == 0) s.dry[ty * s.ntx + tx] = 1;
-      return;
-    }
-  }
+  if (split_faces_settled(s, tx, ty, t)) return;
 
   // state of the tile and its halo (zero outside the grid): b, h, hu, hv
   // copied into b, h, U, V with every copy of the thread in flight at once;
   // once the tile is known to be wet, each thread turns the hu, hv it
   // copied into velocities in place
-  int dryHere = 1;
   for (int q = t; q < SSX * SSY; q += SP_THREADS) {
     const int ly = q / SSX, lx = q - ly * SSX;
     const int gi = i0 - 1 + lx, gj = j0 - 1 + ly;
     if (gi >= 0 && gi < W && gj >= 0 && gj < H) {
       const int k = gj * W + gi;
-      cp_async8(&sm.b[ly][lx], a.b + k);
-      cp_async8(&sm.h[ly][lx], a.h + k);
-      cp_async8(&sm.U[ly][lx], a.hu + k);
-      cp_async8(&sm.V[ly][lx], a.hv + k);
+      cp_async8(&sm.b[ly][lx + TCOL], a.b + k);
+      cp_async8(&sm.h[ly][lx + TCOL], a.h + k);
+      cp_async8(&sm.U[ly][lx + TCOL], a.hu + k);
+      cp_async8(&sm.V[ly][lx + TCOL], a.hv + k);
     } else {
-      sm.b[ly][lx] = 0; sm.h[ly][lx] = 0; sm.U[ly][lx] = 0; sm.V[ly][lx] = 0;
+      sm.b[ly][lx + TCOL] = 0; sm.h[ly][lx + TCOL] = 0; sm.U[ly][lx + TCOL] = 0; sm.V[ly][lx + TCOL] = 0;
     }
   }
   cp_async_wait_all();
+  split_faces_finish(a, s, tx, ty, sm, t);
+}
+
+// The rest of a faces tile once its state tile is in shared memory: the
+// dry test, velocities, slopes and faces.  Every thread of the CTA calls it.
+__device__ __forceinline__ void split_faces_finish(const StageArgs& a, const SplitBufs& s, int tx, int ty,
+                                                   FacesSmem& sm, int t) {
+  const int W = a.W, H = a.H;
+  const int i0 = tx * SPX, j0 = ty * SPY;
+  const double dry = a.minDepth, eps4 = a.eps4;
+  const bool order2 = a.order >= 2;
+  const bool sph = a.sph != 0;
+  const bool bedOn = order2 || sph;
+  int dryHere = 1;
   for (int q = t; q < SSX * SSY; q += SP_THREADS) {
     const int ly = q / SSX, lx = q - ly * SSX;
-    if (!(sm.h[ly][lx] == 0)) dryHere = 0;     // zero outside the grid
+    if (!(sm.h[ly][lx + TCOL] == 0)) dryHere = 0;     // zero outside the grid
   }
   const bool allDry = __syncthreads_and(dryHere) && s.dry && !s.sl[0];
   if (s.dry && t == 0) s.dry[ty * s.ntx + tx] = allDry ? 1 : 0;
@@ -226,7 +253,8 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
     const int ly = q / SSX, lx = q - ly * SSX;
     const int gi = i0 - 1 + lx, gj = j0 - 1 + ly;
     if (gi >= 0 && gi < W && gj >= 0 && gj < H) {
-      const double h = sm.h[ly][lx], hu = sm.U[ly][lx], hv = sm.V[ly][lx];
+      const int c = lx + TCOL;
+      const double h = sm.h[ly][c], hu = sm.U[ly][c], hv = sm.V[ly][c];
       double U, V;
       if (h == 0) {                  // +-0 / den == +-0 and NaN / den == NaN: no division needed
         U = vel_num(hu, h); V = vel_num(hv, h);
@@ -234,7 +262,7 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
         const double den = vel_den(h, eps4);
         U = vel_num(hu, h) / den; V = vel_num(hv, h) / den;
       }
-      sm.U[ly][lx] = U; sm.V[ly][lx] = V;
+      sm.U[ly][c] = U; sm.V[ly][c] = V;
     }
   }
   __syncthreads();
@@ -245,7 +273,7 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
     const int gi = i0 + lx, gj = j0 + ly;
     double sE = 0, sB = 0, sU = 0, sV = 0;
     if (order2 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1) {
-      const int cy = ly + 1, cx = lx + 1;
+      const int cy = ly + 1, cx = lx + 1 + TCOL;
       const double hk = sm.h[cy][cx], hp = sm.h[cy][cx + 1], hm = sm.h[cy][cx - 1];
       if (!(hk <= dry || hp <= dry || hm <= dry)) {
         const double bk = sm.b[cy][cx], bp = sm.b[cy][cx + 1], bm = sm.b[cy][cx - 1];
@@ -265,7 +293,7 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
     const int gi = i0 + lx, gj = j0 + ly;
     double sE = 0, sB = 0, sU = 0, sV = 0;
     if (order2 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1) {
-      const int cy = ly + 1, cx = lx + 1;
+      const int cy = ly + 1, cx = lx + 1 + TCOL;
       const double hk = sm.h[cy][cx], hp = sm.h[cy + 1][cx], hm = sm.h[cy - 1][cx];
       if (!(hk <= dry || hp <= dry || hm <= dry)) {
         const double bk = sm.b[cy][cx], bp = sm.b[cy + 1][cx], bm = sm.b[cy - 1][cx];
@@ -287,6 +315,85 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
   __syncthreads();
 }
 
+// ---- the state tile by tensor-map copies (TMA) --------------------------------
+// One thread issues four 2-D bulk tensor copies (b, h, hu, hv of the stage
+// input) of the box SSXT x SSY at column i0 - 2 (even, so its first element
+// sits on a 16-byte boundary of the row) and row j0 - 1; the copies fill
+// cells outside the grid with zeros, which is what the tile needs there, and
+// complete on an mbarrier the whole CTA waits on.  That replaces the 1540
+// per-element copies and their address arithmetic.  The maps cover this
+// simulation's own device buffers only (no multicast).  Grids whose padded
+// width is odd (a row stride that is not a multiple of 16 bytes) take the
+// per-element path; both give the same bits.
+struct TileMaps { CUtensorMap m[4]; };
+constexpr unsigned TILE_TX_BYTES = 4u * SSY * SSXT * sizeof(double);
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+               "selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(ok)
+               : "r"(smem_addr(bar)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_tile(void* dst, const CUtensorMap* map, int x, int y,
+                                              unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+      ::"r"(smem_addr(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+// Every thread: until the phase `parity` of bar completes, at most `tries`
+// polls (each of which may suspend the thread for a while).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, int tries) {
+  for (int it = 0; it < tries; it++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+constexpr int TMA_WAIT_TRIES = 1 << 22;
+
+// split_faces_tile with the state tile fetched by tensor-map copies.  bar
+// is an initialised mbarrier in shared memory and parity its phase, flipped
+// here for the next tile.  A copy that does not complete within the bound
+// sets bit 4 of Control::status and leaves the tile's faces unwritten.
+__device__ __forceinline__ void split_faces_tile_tma(const StageArgs& a, const SplitBufs& s, int tx, int ty,
+                                                     FacesSmem& sm, const TileMaps& maps,
+                                                     unsigned long long* bar, unsigned& parity, Control* ctl) {
+  const int t = threadIdx.x;
+  if (split_faces_settled(s, tx, ty, t)) return;
+  if (t == 0) {
+    // the generic-proxy accesses of a previous tile come before the copy's writes
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    mbar_expect_tx(bar, TILE_TX_BYTES);
+    const int x = tx * SPX - 2, y = ty * SPY - 1;
+    tma_load_tile(&sm.b[0][0], &maps.m[0], x, y, bar);
+    tma_load_tile(&sm.h[0][0], &maps.m[1], x, y, bar);
+    tma_load_tile(&sm.U[0][0], &maps.m[2], x, y, bar);
+    tma_load_tile(&sm.V[0][0], &maps.m[3], x, y, bar);
+  }
+  const bool ok = mbar_wait_bounded(bar, parity, TMA_WAIT_TRIES);
+  parity ^= 1u;
+  if (!__syncthreads_and(ok)) {                     // uniform: give up on the tile
+    if (t == 0) atomicOr(&ctl->status, 4);
+    mbar_wait_bounded(bar, parity ^ 1u, TMA_WAIT_TRIES);   // let a late copy land first
+    __syncthreads();
+    return;
+  }
+  split_faces_finish(a, s, tx, ty, sm, t);
+}
+
 #ifndef SWE_SPLIT_FACES_MIN_BLOCKS
 #define SWE_SPLIT_FACES_MIN_BLOCKS 4
 #endif
@@ -296,6 +403,19 @@ k_split_faces(StageArgs a, SplitBufs s, Control* ctl) {
   if (ctl->stop) return;
   __shared__ FacesSmem sm;
   split_faces_tile(a, s, blockIdx.x, blockIdx.y, sm);
+}
+
+// The face kernel with its state tile fetched by tensor-map copies.
+__global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_FACES_MIN_BLOCKS)
+k_split_faces_tma(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant__ TileMaps maps) {
+  __shared__ FacesSmem sm;
+  __shared__ alignas(8) unsigned long long bar;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);        // before the wait: touches no global memory
+  pdl_enter();
+  if (ctl->stop) return;
+  __syncthreads();
+  unsigned parity = 0;
+  split_faces_tile_tma(a, s, blockIdx.x, blockIdx.y, sm, maps, &bar, parity, ctl);
 }
 
 struct CellsSmem {
