@@ -227,14 +227,45 @@ __device__ __forceinline__ void split_faces_tile(const StageArgs& a, const Split
       sm.b[ly][lx + TCOL] = 0; sm.h[ly][lx + TCOL] = 0; sm.U[ly][lx + TCOL] = 0; sm.V[ly][lx + TCOL] = 0;
     }
   }
+  if (t < SSY) {                                // column 0 (i0 - 2) is in the box but not needed
+    sm.b[t][0] = 0; sm.h[t][0] = 0; sm.U[t][0] = 0; sm.V[t][0] = 0;
+  }
   cp_async_wait_all();
   split_faces_finish(a, s, tx, ty, sm, t);
 }
 
+// Limited slopes of eta, b, u, v at the state-tile cell (cy, cx) along x
+// (DX = 1) or y (DX = 0), src/swe.mjs:364-411: all four are 0 unless `on`
+// and the cell and both neighbours along the direction are wet.  LIM 0 is
+// the MC limiter inline; LIM -1 the options' limiter chosen at run time.
+// out[q * stride]: the slopes of eta, b, u, v in turn (each stored as soon
+// as it is formed).
+template <int DX, int LIM>
+__device__ __forceinline__ void tile_slopes(const FacesSmem& sm, int lim, double dry, bool on, int cy, int cx,
+                                            double* out, int stride) {
+  constexpr int DY = 1 - DX;
+  const int l = LIM < 0 ? lim : LIM;
+  double sE = 0, sB = 0, sU = 0, sV = 0;
+  if (on) {
+    const double hk = sm.h[cy][cx], hp = sm.h[cy + DY][cx + DX], hm = sm.h[cy - DY][cx - DX];
+    if (!(hk <= dry || hp <= dry || hm <= dry)) {
+      const double bk = sm.b[cy][cx], bp = sm.b[cy + DY][cx + DX], bm = sm.b[cy - DY][cx - DX];
+      sE = limiter(l, (bk + hk) - (bm + hm), (bp + hp) - (bk + hk));
+      sB = limiter(l, bk - bm, bp - bk);
+      const double uk = sm.U[cy][cx];
+      sU = limiter(l, uk - sm.U[cy - DY][cx - DX], sm.U[cy + DY][cx + DX] - uk);
+      const double vk = sm.V[cy][cx];
+      sV = limiter(l, vk - sm.V[cy - DY][cx - DX], sm.V[cy + DY][cx + DX] - vk);
+    }
+  }
+  out[0] = sE; out[stride] = sB; out[2 * stride] = sU; out[3 * stride] = sV;
+}
+
 // The rest of a faces tile once its state tile is in shared memory: the
 // dry test, velocities, slopes and faces.  Every thread of the CTA calls it.
-__device__ __forceinline__ void split_faces_finish(const StageArgs& a, const SplitBufs& s, int tx, int ty,
-                                                   FacesSmem& sm, int t) {
+template <int LIM>
+__device__ __forceinline__ void split_faces_finish_l(const StageArgs& a, const SplitBufs& s, int tx, int ty,
+                                                     FacesSmem& sm, int t) {
   const int W = a.W, H = a.H;
   const int i0 = tx * SPX, j0 = ty * SPY;
   const double dry = a.minDepth, eps4 = a.eps4;
@@ -249,70 +280,53 @@ __device__ __forceinline__ void split_faces_finish(const StageArgs& a, const Spl
   const bool allDry = __syncthreads_and(dryHere) && s.dry && !s.sl[0];
   if (s.dry && t == 0) s.dry[ty * s.ntx + tx] = allDry ? 1 : 0;
   if (allDry) return;                           // uniform across the CTA
-  for (int q = t; q < SSX * SSY; q += SP_THREADS) {
-    const int ly = q / SSX, lx = q - ly * SSX;
-    const int gi = i0 - 1 + lx, gj = j0 - 1 + ly;
-    if (gi >= 0 && gi < W && gj >= 0 && gj < H) {
-      const int c = lx + TCOL;
-      const double h = sm.h[ly][c], hu = sm.U[ly][c], hv = sm.V[ly][c];
-      double U, V;
-      if (h == 0) {                  // +-0 / den == +-0 and NaN / den == NaN: no division needed
-        U = vel_num(hu, h); V = vel_num(hv, h);
-      } else {
-        const double den = vel_den(h, eps4);
-        U = vel_num(hu, h) / den; V = vel_num(hv, h) / den;
-      }
-      sm.U[ly][c] = U; sm.V[ly][c] = V;
+  // velocities over the whole box; a cell outside the grid has h = hu =
+  // hv = 0 there and gets u = v = +0, as it would have kept
+  for (int q = t; q < SSXT * SSY; q += SP_THREADS) {
+    const int ly = q / SSXT, c = q - ly * SSXT;
+    const double h = sm.h[ly][c], hu = sm.U[ly][c], hv = sm.V[ly][c];
+    double U, V;
+    if (h == 0) {                  // +-0 / den == +-0 and NaN / den == NaN: no division needed
+      U = vel_num(hu, h); V = vel_num(hv, h);
+    } else {
+      const double den = vel_den(h, eps4);
+      U = vel_num(hu, h) / den; V = vel_num(hv, h) / den;
     }
+    sm.U[ly][c] = U; sm.V[ly][c] = V;
   }
   __syncthreads();
 
-  // x slopes (src/swe.mjs:364-411, d = 0)
-  for (int q = t; q < SPY * (SPX + 1); q += SP_THREADS) {
-    const int ly = q / (SPX + 1), lx = q - ly * (SPX + 1);
-    const int gi = i0 + lx, gj = j0 + ly;
-    double sE = 0, sB = 0, sU = 0, sV = 0;
-    if (order2 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1) {
-      const int cy = ly + 1, cx = lx + 1 + TCOL;
-      const double hk = sm.h[cy][cx], hp = sm.h[cy][cx + 1], hm = sm.h[cy][cx - 1];
-      if (!(hk <= dry || hp <= dry || hm <= dry)) {
-        const double bk = sm.b[cy][cx], bp = sm.b[cy][cx + 1], bm = sm.b[cy][cx - 1];
-        const double eC = bk + hk, eP = bp + hp, eM = bm + hm;
-        const double uk = sm.U[cy][cx], vk = sm.V[cy][cx];
-        sE = limiter(a.lim, eC - eM, eP - eC);
-        sB = limiter(a.lim, bk - bm, bp - bk);
-        sU = limiter(a.lim, uk - sm.U[cy][cx - 1], sm.U[cy][cx + 1] - uk);
-        sV = limiter(a.lim, vk - sm.V[cy][cx - 1], sm.V[cy][cx + 1] - vk);
-      }
-    }
-    sm.xs[0][ly][lx] = sE; sm.xs[1][ly][lx] = sB; sm.xs[2][ly][lx] = sU; sm.xs[3][ly][lx] = sV;
-  }
-  // y slopes (d = 1)
-  for (int q = t; q < (SPY + 1) * SPX; q += SP_THREADS) {
-    const int ly = q / SPX, lx = q - ly * SPX;
-    const int gi = i0 + lx, gj = j0 + ly;
-    double sE = 0, sB = 0, sU = 0, sV = 0;
-    if (order2 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1) {
-      const int cy = ly + 1, cx = lx + 1 + TCOL;
-      const double hk = sm.h[cy][cx], hp = sm.h[cy + 1][cx], hm = sm.h[cy - 1][cx];
-      if (!(hk <= dry || hp <= dry || hm <= dry)) {
-        const double bk = sm.b[cy][cx], bp = sm.b[cy + 1][cx], bm = sm.b[cy - 1][cx];
-        const double eC = bk + hk, eP = bp + hp, eM = bm + hm;
-        const double uk = sm.U[cy][cx], vk = sm.V[cy][cx];
-        sE = limiter(a.lim, eC - eM, eP - eC);
-        sB = limiter(a.lim, bk - bm, bp - bk);
-        sU = limiter(a.lim, uk - sm.U[cy - 1][cx], sm.U[cy + 1][cx] - uk);
-        sV = limiter(a.lim, vk - sm.V[cy - 1][cx], sm.V[cy + 1][cx] - vk);
-      }
-    }
-    sm.ys[0][ly][lx] = sE; sm.ys[1][ly][lx] = sB; sm.ys[2][ly][lx] = sU; sm.ys[3][ly][lx] = sV;
-  }
-  __syncthreads();
-
+  // slopes (src/swe.mjs:364-411): each thread its own cell in x and y; the
+  // east column's x slopes (the first SPY threads) and the north row's y
+  // slopes (the second warp) besides
   const int lx = t % SPX, ly = t / SPX;
   const int gi = i0 + lx, gj = j0 + ly;
+  constexpr int XS = SPY * (SPX + 1), YS = (SPY + 1) * SPX;   // strides of xs[q], ys[q]
+  {
+    const bool on = order2 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1;
+    const int cy = ly + 1, cx = lx + 1 + TCOL;
+    tile_slopes<1, LIM>(sm, a.lim, dry, on, cy, cx, &sm.xs[0][ly][lx], XS);
+    tile_slopes<0, LIM>(sm, a.lim, dry, on, cy, cx, &sm.ys[0][ly][lx], YS);
+  }
+  if (t < SPY) {                                // x slopes of column i0 + SPX, row j0 + t
+    const int ei = i0 + SPX, ej = j0 + t;
+    const bool on = order2 && ej >= 1 && ej < H - 1 && ei >= 1 && ei < W - 1;
+    tile_slopes<1, LIM>(sm, a.lim, dry, on, t + 1, SPX + 1 + TCOL, &sm.xs[0][t][SPX], XS);
+  } else if (t >= 32 && t < 32 + SPX) {         // y slopes of row j0 + SPY, column i0 + t - 32
+    const int c = t - 32, ni = i0 + c, nj = j0 + SPY;
+    const bool on = order2 && nj >= 1 && nj < H - 1 && ni >= 1 && ni < W - 1;
+    tile_slopes<0, LIM>(sm, a.lim, dry, on, SPY + 1, c + 1 + TCOL, &sm.ys[0][SPY][c], YS);
+  }
+  __syncthreads();
+
   if (gi < W && gj < H) split_faces_cell(a, s, sm, lx, ly, gi, gj, sph, bedOn);
   __syncthreads();
+}
+
+__device__ __forceinline__ void split_faces_finish(const StageArgs& a, const SplitBufs& s, int tx, int ty,
+                                                   FacesSmem& sm, int t) {
+  if (a.lim == 0) split_faces_finish_l<0>(a, s, tx, ty, sm, t);    // mc, the default
+  else split_faces_finish_l<-1>(a, s, tx, ty, sm, t);
 }
 
 // ---- the state tile by tensor-map copies (TMA) --------------------------------
