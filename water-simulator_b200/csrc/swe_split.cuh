@@ -435,12 +435,6 @@ k_split_faces_tma(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant_
 struct CellsSmem {
   double st[6][SP_THREADS];       // each thread's own cell: h, hu, hv, then U0 (stage 2)
   double th[SPY + 2][SPX + 2];
-  // mass fluxes of the x faces of cols i0-2 .. i0+32, rows j0-1 .. j0+8, and
-  // of the y faces of cols i0-1 .. i0+32, rows j0-2 .. j0+8 (each face
-  // indexed by its left / lower cell): everything the limiter of the tile
-  // and its ring and the gather of the tile read
-  double mx[SPY + 2][SPX + 3];
-  double my[SPY + 3][SPX + 2];
   double red[2][SP_THREADS / 32];
   int dry[3][3];                  // dry flags of the tile's 3 x 3 neighbourhood
   int prev;                       // the output tile's record as this kernel left it last time
@@ -458,40 +452,15 @@ __device__ __forceinline__ double split_load(const CellsSmem& sm, int i0, int j0
 
 // Positivity limiter of cell (gi, gj) from its four faces' mass fluxes
 // (src/swe.mjs:511-529), with the same conservative pre-test as stage_tile.
-// The mass fluxes the tile's limiter and gather read, staged once in shared
-// memory (row segments: coalesced), +0 where the owning tile was dry or
-// the face lies outside the grid -- the values split_load would give.
-__device__ __forceinline__ void split_stage_mass(const StageArgs& a, const SplitBufs& s, CellsSmem& sm,
-                                                 int i0, int j0, int t) {
-  const int W = a.W, H = a.H;
-  for (int q = t; q < (SPY + 2) * (SPX + 3); q += SP_THREADS) {
-    const int ly = q / (SPX + 3), lx = q - ly * (SPX + 3);
-    const int gi = i0 - 2 + lx, gj = j0 - 1 + ly;
-    double v = 0;
-    if (gi >= 0 && gi < W && gj >= 0 && gj < H) v = split_load(sm, i0, j0, gi, gj, s.fx[F_M], gj * W + gi);
-    sm.mx[ly][lx] = v;
-  }
-  for (int q = t; q < (SPY + 3) * (SPX + 2); q += SP_THREADS) {
-    const int ly = q / (SPX + 2), lx = q - ly * (SPX + 2);
-    const int gi = i0 - 1 + lx, gj = j0 - 2 + ly;
-    double v = 0;
-    if (gi >= 0 && gi < W && gj >= 0 && gj < H) v = split_load(sm, i0, j0, gi, gj, s.fy[F_M], gj * W + gi);
-    sm.my[ly][lx] = v;
-  }
-}
-
-// (rx, ry): the cell's place in the one-cell ring around the tile (gi =
-// i0 - 1 + rx, gj = j0 - 1 + ry); its four mass fluxes come from the staged
-// sm.mx / sm.my (split_stage_mass).
-__device__ __forceinline__ double split_theta(const StageArgs& a, const CellsSmem& sm, double dt, int gi, int gj,
-                                              int rx, int ry) {
+__device__ __forceinline__ double split_theta(const StageArgs& a, const SplitBufs& s, const CellsSmem& sm,
+                                              int i0, int j0, double dt, int gi, int gj) {
   const int W = a.W, H = a.H;
   if (!(dt > 0 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1)) return 1;
   const int k = gj * W + gi;
-  const double fxE = sm.mx[ry][rx + 1];
-  const double fxW = sm.mx[ry][rx];
-  const double fyN = sm.my[ry + 1][rx];
-  const double fyS = sm.my[ry][rx];
+  const double fxE = split_load(sm, i0, j0, gi, gj, s.fx[F_M], k);
+  const double fxW = split_load(sm, i0, j0, gi - 1, gj, s.fx[F_M], k - 1);
+  const double fyN = split_load(sm, i0, j0, gi, gj, s.fy[F_M], k);
+  const double fyS = split_load(sm, i0, j0, gi, gj - 1, s.fy[F_M], k - W);
   const double avail = a.h[k];
   const double est = ((fxE > 0 ? fxE : 0) - (fxW < 0 ? fxW : 0)) * a.m.rdxRow[gj]
                    + (fyN > 0 ? fyN : 0) * a.m.rdyRowN[gj] - (fyS < 0 ? fyS : 0) * a.m.rdyRowS[gj];
@@ -584,11 +553,10 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
   const bool interior = colY && rowX;
   double wM = 0, wT = 0, wN = 0, eM = 0, eT = 0, eN = 0, sM = 0, sT = 0, sN = 0, nM = 0, nT = 0, nN = 0;
   const bool dW = sm.dry[1][lx == 0 ? 0 : 1], dS = sm.dry[ly == 0 ? 0 : 1][1], dC = sm.dry[1][1];
-  // mass fluxes from the staged copies (+0 for a dry tile, as a load would be)
-  if (!DRY && hasW && !dW) { wM = sm.mx[ly + 1][lx + 1]; wT = s.fx[F_T][k - 1]; wN = s.fx[F_NPR][k - 1]; }
-  if (!DRY && hasE && !dC) { eM = sm.mx[ly + 1][lx + 2]; eT = s.fx[F_T][k]; eN = s.fx[F_NPL][k]; }
-  if (!DRY && hasS && !dS) { sM = sm.my[ly + 1][lx + 1]; sT = s.fy[F_T][k - W]; sN = s.fy[F_NPR][k - W]; }
-  if (!DRY && hasN && !dC) { nM = sm.my[ly + 2][lx + 1]; nT = s.fy[F_T][k]; nN = s.fy[F_NPL][k]; }
+  if (!DRY && hasW && !dW) { wM = s.fx[F_M][k - 1]; wT = s.fx[F_T][k - 1]; wN = s.fx[F_NPR][k - 1]; }
+  if (!DRY && hasE && !dC) { eM = s.fx[F_M][k]; eT = s.fx[F_T][k]; eN = s.fx[F_NPL][k]; }
+  if (!DRY && hasS && !dS) { sM = s.fy[F_M][k - W]; sT = s.fy[F_T][k - W]; sN = s.fy[F_NPR][k - W]; }
+  if (!DRY && hasN && !dC) { nM = s.fy[F_M][k]; nT = s.fy[F_T][k]; nN = s.fy[F_NPL][k]; }
   cp_async_wait_all();
   const double hin = sm.st[0][t], huin = sm.st[1][t], hvin = sm.st[2][t];
   double tb0 = 0, tb1 = 0, tg = 0, Uk = 0;
@@ -796,11 +764,9 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
     }
   }
   if (!fold) {
-    split_stage_mass(a, s, sm, i0, j0, t);
-    __syncthreads();
     for (int q = t; q < (SPX + 2) * (SPY + 2); q += SP_THREADS) {
       const int ly = q / (SPX + 2), lx = q - ly * (SPX + 2);
-      sm.th[ly][lx] = allDry ? 1.0 : split_theta(a, sm, dt, i0 - 1 + lx, j0 - 1 + ly, lx, ly);
+      sm.th[ly][lx] = allDry ? 1.0 : split_theta(a, s, sm, i0, j0, dt, i0 - 1 + lx, j0 - 1 + ly);
     }
     __syncthreads();
   }
