@@ -52,7 +52,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true",
                    help="leave out the all-wet, batched-ensemble and adjoint objects of the 1-GPU line")
-    p.add_argument("--workload", default="beach", choices=["beach", "ensemble", "adjoint", "sphere", "slabs"],
+    p.add_argument("--workload", default="beach",
+                   choices=["beach", "ensemble", "adjoint", "sphere", "slabs", "allwet"],
                    help="beach: the 2048x2048 headline; ensemble: the 256-basin batched form vs the plain "
                         "kernel; sphere: the 1440x720 tide; adjoint: the 1024x1024 misfit gradient; slabs: "
                         "the beach cut into row slabs over the ranks (device halo exchange)")
@@ -255,7 +256,7 @@ def stream_of(swe, sim):
     return sp.value
 
 
-def all_wet_summary(torch, swe, steps, device=0):
+def all_wet_summary(torch, swe, steps, device=0, warm=32):
     """An all-wet 2048 x 2048 grid (bump + roughness bed, dam break 3.0 /
     2.5 m, Manning 0.03, walls): every tile computes every cell, so this is
     the rate of the wet-cell kernels, with the roofline of the stage-2 pair."""
@@ -265,7 +266,7 @@ def all_wet_summary(torch, swe, steps, device=0):
     X, _ = _centres(n, n, DX)
     eta = np.where(X < n * DX / 2, 3.0, 2.5)
     sim = swe.ShallowWater(nx=n, ny=n, dx=DX, bed=b, eta0=eta, manning=MANNING)
-    sim.run(32)
+    sim.run(warm)
     sim.synchronize()
     done, ms, clocks = timed_on(torch, stream_of(swe, sim), lambda: sim.run(steps), device)
     if done != steps:
@@ -906,6 +907,15 @@ def main():
         return run_sphere(args)
     if args.workload == "slabs":
         return run_slabs(args)
+    if args.workload == "allwet":
+        import torch
+        import __graft_entry__
+        swe = __graft_entry__.load_package()
+        line = all_wet_summary(torch, swe, args.steps, 0, warm=max(args.warmup, 3))
+        line.update(metric="FP64 cell-updates/s, all-wet 2048x2048", n_gpus=1, warmup=args.warmup,
+                    higher_is_better=True, dtype="f64", data="synthetic (seeded)")
+        print(json.dumps(line))
+        return 0
     return run_ours(args)
 
 

@@ -9,7 +9,10 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libswe_b200.so")
+# The exact build (-fmad=false, bit-identical to the oracle) by default;
+# SWE_B200_ARITH=fma selects the build whose compiler fuses multiply-adds.
+LIB_PATH = os.path.join(HERE, "libswe_b200_fma.so" if os.environ.get("SWE_B200_ARITH") == "fma"
+                        else "libswe_b200.so")
 
 SWE_OK, SWE_EINVAL, SWE_ECUDA, SWE_ENONFINITE, SWE_ETIMEOUT = 0, -1, -2, -3, -4
 

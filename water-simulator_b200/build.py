@@ -1,8 +1,14 @@
-"""Build libswe_b200.so (sm_100a, FP64) in-tree with nvcc.
+"""Build the library (sm_100a, FP64) in-tree with nvcc, in two arithmetic
+modes from the same sources:
 
-The library is compiled with -fmad=false: no multiply-add is contracted, so
-the device arithmetic rounds operation by operation like the reference's
-JavaScript engine (the parity build of the step).
+  libswe_b200.so      -fmad=false: no multiply-add is contracted, so the
+                      device arithmetic rounds operation by operation like
+                      the reference's JavaScript engine -- the comparison
+                      build, bit-identical to the oracle; the default.
+  libswe_b200_fma.so  -fmad=true: the compiler fuses multiply-adds (one
+                      rounding instead of two); results agree with the
+                      comparison build to round-off (held to 1e-12 per field
+                      per step by the tests).  Chosen with SWE_B200_ARITH=fma.
 """
 import glob
 import os
@@ -10,7 +16,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB = os.path.join(HERE, "libswe_b200.so")
+VARIANTS = {"exact": ("libswe_b200.so", "-fmad=false"), "fma": ("libswe_b200_fma.so", "-fmad=true")}
+LIB = os.path.join(HERE, VARIANTS["exact"][0])
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("swe_api.cu", "swe_batch.cu", "swe_adjoint.cu",
                                                     "swe_noalloc.cu", "swe_gridlands.cu", "swe_render.cu")]
 DEPS = SOURCES + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [
@@ -18,7 +25,7 @@ DEPS = SOURCES + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-fmad=false", "-lineinfo", "-std=c++17",
+    "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC", "-shared",
 ]
 
@@ -28,23 +35,32 @@ def nvcc():
     return cand if os.path.exists(cand) else "nvcc"
 
 
-def up_to_date():
-    if not os.path.exists(LIB):
+def lib_path(variant="exact"):
+    return os.path.join(HERE, VARIANTS[variant][0])
+
+
+def up_to_date(path):
+    if not os.path.exists(path):
         return False
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(path)
     return all(os.path.getmtime(d) <= t for d in DEPS if os.path.exists(d))
 
 
-def build_library(force=False, verbose=False, extra=()):
-    """Compile the C-ABI library; returns its path."""
-    if not force and up_to_date():
-        return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ["-o", LIB] + SOURCES
+def build_library(force=False, verbose=False, extra=(), variant="exact"):
+    """Compile one arithmetic mode of the C-ABI library; returns its path."""
+    path = lib_path(variant)
+    if not force and up_to_date(path):
+        return path
+    cmd = [nvcc()] + NVCC_FLAGS + [VARIANTS[variant][1]] + list(extra) + ["-o", path] + SOURCES
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True, cwd=HERE)
-    return LIB
+    return path
+
+
+def build_all(force=False, verbose=False):
+    return [build_library(force, verbose, variant=v) for v in VARIANTS]
 
 
 if __name__ == "__main__":
-    print(build_library(force="--force" in sys.argv, verbose=True))
+    print(build_all(force="--force" in sys.argv, verbose=True))

@@ -975,7 +975,10 @@ int swe_run(swe_sim* s, int n, double dt_fixed, double t_end, int* done) {
   const double steps0 = s->steps;
   const int mode = dt_fixed > 0 ? 2 : 3;
   const double dtv = dt_fixed > 0 ? dt_fixed : 0;
-  const int chunk = std::min(n, 32);
+  // Graphs of 32 steps; a shorter run (or remainder) is launched step by
+  // step: a graph of 20 steps measured 12% slower per step than the same
+  // steps launched directly, one of 32 as fast as them.
+  const int chunk = 32;
   // The graph of `chunk` steps with the current value of s->settle, built
   // once per (chunk, mode, dt, tEnd, options) and kept.
   auto graph_for = [&](cudaGraphExec_t* out) -> int {
