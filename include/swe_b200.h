@@ -297,8 +297,9 @@ int swe_batch_get_scalar(swe_batch* s, int basin, int which, double* out);  /* T
  * Gradient of a gauge misfit J = sum_steps sum_gauges (eta - obs)^2 with
  * respect to the bed b and the per-cell Manning n (both over the padded
  * grid; ghosts get 0), for `steps` self-timed steps from still water eta0
- * (h = max(0, eta0 - b), src/swe.mjs:229-231).  Cartesian, walls on every
- * side.  The forward pass records dt and checkpoints the state every
+ * (h = max(0, eta0 - b), src/swe.mjs:229-231).  Cartesian; walls on every
+ * side unless swe_adjoint_set_boundary says otherwise.  The forward pass
+ * records dt and checkpoints the state every
  * `checkpoint_every` steps; swe_adjoint_backward recomputes each segment
  * and runs the hand-written reverse of every step, branches fixed as taken.
  * gauge_cells are padded indices k = j*W + i.  manning_field may be NULL
@@ -316,6 +317,15 @@ int swe_adjoint_backward(swe_adjoint* s, double* grad_b, double* grad_n);
  * (a finite-difference check needs the same frozen dts). */
 int swe_adjoint_dt_sequence(swe_adjoint* s, double* dts_out, const double* dts_in);
 int swe_adjoint_get_stream(swe_adjoint* s, void** stream);
+/* The boundary of one side (SWE_SIDE_*) for the forward and its reverse:
+ * SWE_BC_REFLECT (the default), _OUTFLOW, _PERIODIC, or _FLATHER with the
+ * exterior state of swe_adjoint_set_flather_values (initially eta = u = 0),
+ * as swe_set_boundary does for a simulation (src/swe.mjs:1026-1126).  A set
+ * boundary asks for a new forward pass before the next backward. */
+int swe_adjoint_set_boundary(swe_adjoint* s, int side, int kind);
+/* Flather on `side` with the constant exterior surface eta_ext and normal
+ * velocity u_ext (src/swe.mjs:1085-1115; a tide signal is not covered). */
+int swe_adjoint_set_flather_values(swe_adjoint* s, int side, double eta_ext, double u_ext);
 
 /* ---- stage kernels -----------------------------------------------------------
  * Two implementations of each SSP-RK2 stage, bit-identical in their results:

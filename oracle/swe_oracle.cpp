@@ -937,13 +937,37 @@ void   oracle_hllc(double* out3, double hL, double huL, double hvL, double hR, d
 // (bed) and dn (Manning field; NULL n means the scalar o->manning).  dt is
 // each step's maxDt() of the value part, held as a constant, as the adjoint
 // holds it.  Returns J, dJ = <grad J, (db, dn)>, and the dt sequence.
+// oracle_tlm_misfit_bc: the same with a boundary kind per side (W, E, S, N:
+// OB_REFLECT, OB_OUTFLOW, OB_PERIODIC, OB_FLATHER) and, for Flather sides,
+// the constant exterior surface and normal velocity.
+int oracle_tlm_misfit_bc(const oracle_options* o, const double* b, const double* eta0, const double* n,
+                         const double* db, const double* dn, int ng, const int* gauges, int steps,
+                         const double* obs, int threads, const int* kinds, const double* fl_eta,
+                         const double* fl_u, double* J, double* dJ, double* dts);
+
 int oracle_tlm_misfit(const oracle_options* o, const double* b, const double* eta0, const double* n,
                       const double* db, const double* dn, int ng, const int* gauges, int steps,
                       const double* obs, int threads, double* J, double* dJ, double* dts) {
+  return oracle_tlm_misfit_bc(o, b, eta0, n, db, dn, ng, gauges, steps, obs, threads, nullptr, nullptr, nullptr,
+                              J, dJ, dts);
+}
+
+int oracle_tlm_misfit_bc(const oracle_options* o, const double* b, const double* eta0, const double* n,
+                         const double* db, const double* dn, int ng, const int* gauges, int steps,
+                         const double* obs, int threads, const int* kinds, const double* fl_eta,
+                         const double* fl_u, double* J, double* dJ, double* dts) {
   if (!o || o->sphere || !b || !eta0 || !db || ng < 1 || !gauges || steps < 1 || !obs) {
     g_err = "oracle_tlm_misfit: Cartesian options, b, eta0, db, gauges, steps, obs"; return -1;
   }
   SimT<Dual> s;
+  for (int q = 0; q < 4; q++) {
+    const int kind = kinds ? kinds[q] : OB_REFLECT;
+    if (kind < OB_REFLECT || kind > OB_FLATHER) { g_err = "oracle_tlm_misfit_bc: bad boundary kind"; return -1; }
+    s.bc[q] = kind;
+    s.flTide[q] = false;
+    s.flEta[q] = fl_eta ? fl_eta[q] : 0.0;
+    s.flU[q] = fl_u ? fl_u[q] : 0.0;
+  }
   s.nx = o->nx; s.ny = o->ny; s.ng = 2; s.W = s.nx + 4; s.H = s.ny + 4; s.N = s.W * s.H;
   s.dx = o->dx; s.dy = o->dy; s.manning = o->manning; s.minDepth = o->min_depth; s.cfl = o->cfl;
   s.coriolis = o->coriolis; s.eps4 = std::pow(jmax(o->min_depth, 1e-12), 4.0);

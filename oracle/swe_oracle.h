@@ -86,6 +86,12 @@ void         oracle_hllc(double* out3, double hL, double huL, double hvL, double
 int          oracle_tlm_misfit(const oracle_options* o, const double* b, const double* eta0, const double* n,
                                const double* db, const double* dn, int ng, const int* gauges, int steps,
                                const double* obs, int threads, double* J, double* dJ, double* dts);
+/* The same with a boundary kind per side (W, E, S, N; NULL: reflect) and the
+ * constant Flather exterior surface and normal velocity (NULL: 0). */
+int          oracle_tlm_misfit_bc(const oracle_options* o, const double* b, const double* eta0, const double* n,
+                                  const double* db, const double* dn, int ng, const int* gauges, int steps,
+                                  const double* obs, int threads, const int* kinds, const double* fl_eta,
+                                  const double* fl_u, double* J, double* dJ, double* dts);
 
 #ifdef __cplusplus
 }

@@ -20,10 +20,11 @@ sys.path.insert(0, HERE)
 import numpy as np  # noqa: E402
 
 import __graft_entry__  # noqa: E402
+
+swe = __graft_entry__.load_package()        # registers the package scenarios imports from
+
 from oracle_sim import OracleSim  # noqa: E402
 import scenarios as S  # noqa: E402
-
-swe = __graft_entry__.load_package()
 THREADS = os.cpu_count() or 1
 
 

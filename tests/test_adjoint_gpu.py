@@ -103,3 +103,51 @@ def test_gauges_sharing_a_cell(swe):
     got = float(np.dot(gb, db.reshape(-1)) + np.dot(gn, dn.reshape(-1)))
     assert abs(got - dJ) <= 1e-8 * abs(dJ), (got, dJ)
     adj.close()
+
+
+BOUNDARY_CASES = {
+    "outflow_we": {"west": "outflow", "east": "outflow"},
+    "periodic_all": {"west": "periodic", "east": "periodic", "south": "periodic", "north": "periodic"},
+    "flather_west": {"west": ("flather", 2.05, 0.0), "east": "outflow"},
+    "flather_sn_periodic_we": {"south": ("flather", 2.0, 0.01), "north": ("flather", 1.95, -0.02),
+                               "west": "periodic", "east": "periodic"},
+    "mixed": {"east": ("flather", 2.0, 0.0), "south": "outflow", "north": "periodic"},
+}
+
+
+@pytest.mark.parametrize("name", list(BOUNDARY_CASES))
+def test_adjoint_boundaries_match_tangent_linear(swe, name):
+    """Outflow, periodic and Flather sides (src/swe.mjs:1026-1126): the
+    forward equals the oracle's, the gradient its tangent-linear model."""
+    from water_simulator_b200 import workloads
+    bcs = BOUNDARY_CASES[name]
+    steps, nx, ny = 24, 40, 30
+    c = workloads.adjoint_case(nx=nx, ny=ny, dx=10.0, n_gauges=6, seed=31, hump=0.4)
+    kw = dict(manning_field=c["n"], gauges=c["gauges"], steps=steps, checkpoint_every=7, boundaries=bcs)
+    truth = swe.MisfitAdjoint(nx, ny, 10.0, c["b_true"], c["eta0"], **kw)
+    _, obs = truth.forward()
+    truth.close()
+    adj = swe.MisfitAdjoint(nx, ny, 10.0, c["b"], c["eta0"], **kw)
+    adj.set_observations(obs)
+    J, _ = adj.forward()
+    gb, gn = adj.backward()
+    rng = np.random.default_rng(5)
+    for trial in range(3):
+        db = rng.normal(0, 1, c["b"].shape)
+        dn = rng.normal(0, 1e-3, c["n"].shape) if trial else np.zeros(c["n"].shape)
+        Jt, dJ, _ = tlm_misfit(c, c["b"], c["n"], db, dn, steps, obs, bcs=bcs)
+        assert abs(Jt - J) <= 1e-12 * abs(J), (name, Jt, J)
+        got = float(np.dot(gb, db.reshape(-1)) + np.dot(gn, dn.reshape(-1)))
+        assert abs(got - dJ) <= 1e-8 * abs(dJ), (name, trial, got, dJ)
+    g2 = gb.reshape(ny + 4, nx + 4)
+    assert np.all(g2[:2] == 0) and np.all(g2[-2:] == 0) and np.all(g2[:, :2] == 0) and np.all(g2[:, -2:] == 0)
+    adj.close()
+
+
+def test_adjoint_boundary_refusals(swe):
+    c = swe.MisfitAdjoint(8, 8, 10.0, np.zeros(144), 1.0, gauges=[50], steps=2)
+    with pytest.raises(ValueError):
+        c.set_boundary("west", "sponge")
+    with pytest.raises(KeyError):
+        c.set_boundary("up", "reflect")
+    c.close()

@@ -358,6 +358,40 @@ def test_hllc_batch_bit_identical(swe):
     assert out[0] == 2 * math.sqrt(S.G_REF * 0.5) * 0.5 / 3 or abs(out[0] - 2 * math.sqrt(S.G_REF * 0.5) * 0.5 / 3) < 1e-15
 
 
+def _same_bits(a, b):
+    """Equal as 64-bit patterns, or both NaN (NaN payloads are not compared)."""
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return bool(np.all((a.view(np.int64) == b.view(np.int64)) | (np.isnan(a) & np.isnan(b))))
+
+
+def test_zero_dividends_bit_identical(swe):
+    """Still water: the momenta are +-0, and the divisions by h and by the
+    velocity denominator take their zero-dividend form on the device.  The
+    signs of the zero results, and infinite, NaN and zero depths, as the
+    oracle gives them."""
+    z = [0.0, -0.0]
+    depths = [0.5, 2.0, 1.5e-3, 1e-300, 1e300, math.inf, math.nan, 0.0, -0.0, -1.0]
+    rows = []
+    for hL in depths:
+        for hR in (0.5, 2.0, hL):
+            for a in z:
+                for b in z:
+                    rows.append([hL, a, b, hR, b, a, 1e-3])
+                    rows.append([hL, a * hL if math.isfinite(hL) else a, 1.0, hR, 0.25, b, 1e-3])
+    rows = np.array(rows)
+    got = swe.hllc_batch(rows)
+    for q in range(len(rows)):
+        want = oracle_hllc(*rows[q])
+        assert _same_bits(got[q], want), (q, rows[q], got[q], want)
+    sim = swe.ShallowWater(nx=4, ny=4, dx=1, bed=lambda x, y: -1, eta0=0)
+    ref = OracleSim(nx=4, ny=4, dx=1, bed=lambda x, y: -1, eta0=0)
+    hq = np.array([0.0, -0.0] * len(depths))
+    hh = np.repeat(depths, 2)
+    got = sim.vel(hq, hh)
+    want = [ref.vel(float(a), float(b)) for a, b in zip(hq, hh)]
+    assert _same_bits(got, want), (got, want)
+
+
 def test_vel_exact(swe):
     sim = swe.ShallowWater(nx=4, ny=4, dx=1, bed=lambda x, y: -1, eta0=0)
     ref = OracleSim(nx=4, ny=4, dx=1, bed=lambda x, y: -1, eta0=0)

@@ -31,3 +31,23 @@ def test_tlm_matches_central_differences():
             Jm = oracle_misfit(case, case["b"] - eps * db, case["n"] - eps * dn, steps, obs, dts)
             errs.append(abs((Jp - Jm) / (2 * eps) - dJ) / abs(dJ))
         assert min(errs) <= 1e-5, (trial, errs)
+
+
+def test_tlm_with_open_boundaries_matches_central_differences():
+    """The same with outflow, periodic and constant-state Flather sides."""
+    case = small_case()
+    steps = 20
+    rng = np.random.default_rng(4)
+    obs = rng.normal(2.0, 0.05, (steps, len(case["gauges"])))
+    for bcs in ({"west": ("flather", 2.05, 0.0), "east": "outflow", "south": "periodic", "north": "periodic"},
+                {"south": ("flather", 1.95, -0.02), "north": "outflow", "west": "periodic", "east": "periodic"}):
+        db = rng.normal(0, 1, case["b"].shape)
+        dn = rng.normal(0, 1e-3, case["n"].shape)
+        J, dJ, dts = tlm_misfit(case, case["b"], case["n"], db, dn, steps, obs, bcs=bcs)
+        assert J == oracle_misfit(case, case["b"], case["n"], steps, obs, dts, bcs=bcs)
+        errs = []
+        for eps in (1e-4, 1e-5, 1e-6, 1e-7):
+            Jp = oracle_misfit(case, case["b"] + eps * db, case["n"] + eps * dn, steps, obs, dts, bcs=bcs)
+            Jm = oracle_misfit(case, case["b"] - eps * db, case["n"] - eps * dn, steps, obs, dts, bcs=bcs)
+            errs.append(abs((Jp - Jm) / (2 * eps) - dJ) / abs(dJ))
+        assert min(errs) <= 1e-5, (bcs, errs)

@@ -7,11 +7,29 @@ import numpy as np
 from oracle_sim import OracleOptions, OracleSim, oracle_lib, _dp
 
 
-def tlm_misfit(case, b, n, db, dn, steps, obs, threads=1):
+SIDE_ORDER = ("west", "east", "south", "north")
+KIND = {"reflect": 0, "outflow": 1, "periodic": 2, "flather": 3}
+
+
+def boundary_arrays(bcs):
+    """(kinds, flather eta, flather u) in W, E, S, N order from a dict of
+    side -> "reflect" | "outflow" | "periodic" | ("flather", eta, u)."""
+    kinds, fe, fu = [0] * 4, [0.0] * 4, [0.0] * 4
+    for side, bc in (bcs or {}).items():
+        q = SIDE_ORDER.index(side)
+        if isinstance(bc, str):
+            kinds[q] = KIND[bc]
+        else:
+            kinds[q], fe[q], fu[q] = KIND["flather"], float(bc[1]), float(bc[2])
+    return kinds, fe, fu
+
+
+def tlm_misfit(case, b, n, db, dn, steps, obs, threads=1, bcs=None):
     lib = oracle_lib()
-    fn = lib.oracle_tlm_misfit
+    fn = lib.oracle_tlm_misfit_bc
     D, I, DP = ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
-    fn.argtypes = [ctypes.POINTER(OracleOptions), DP, DP, DP, DP, DP, I, ctypes.POINTER(ctypes.c_int), I, DP, I,
+    IP = ctypes.POINTER(ctypes.c_int)
+    fn.argtypes = [ctypes.POINTER(OracleOptions), DP, DP, DP, DP, DP, I, IP, I, DP, I, IP, DP, DP,
                    ctypes.POINTER(D), ctypes.POINTER(D), DP]
     fn.restype = I
     o = OracleOptions()
@@ -22,17 +40,29 @@ def tlm_misfit(case, b, n, db, dn, steps, obs, threads=1):
     ob = np.ascontiguousarray(obs, dtype=np.float64).reshape(-1)
     J, dJ = D(), D()
     dts = np.zeros(steps)
+    kinds, fe, fu = boundary_arrays(bcs)
+    ka = np.ascontiguousarray(kinds, dtype=np.int32)
+    fe, fu = np.ascontiguousarray(fe), np.ascontiguousarray(fu)
     rc = fn(ctypes.byref(o), _dp(arrs[0]), _dp(arrs[1]), _dp(arrs[2]), _dp(arrs[3]), _dp(arrs[4]), len(g),
-            g.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), steps, _dp(ob), threads, ctypes.byref(J),
-            ctypes.byref(dJ), _dp(dts))
+            g.ctypes.data_as(IP), steps, _dp(ob), threads, ka.ctypes.data_as(IP), _dp(fe), _dp(fu),
+            ctypes.byref(J), ctypes.byref(dJ), _dp(dts))
     assert rc == 0, lib.oracle_last_error()
     return J.value, dJ.value, dts
 
 
-def oracle_misfit(case, b, n, steps, obs, dts):
+def oracle_misfit(case, b, n, steps, obs, dts, bcs=None):
     """J on the oracle (doubles) with the dt sequence held fixed."""
     sim = OracleSim(nx=case["nx"], ny=case["ny"], dx=case["dx"], bed=np.asarray(b), eta0=case["eta0"], manning=0.025)
     sim.setManningField(n)
+    if bcs:
+        conv = {}
+        for side, bc in bcs.items():
+            if isinstance(bc, str):
+                conv[side] = bc
+            else:
+                e, u = float(bc[1]), float(bc[2])
+                conv[side] = ("flather", lambda t, e=e: e, lambda t, u=u: u)
+        sim.set_boundaries(**conv)
     J = 0.0
     g = case["gauges"]
     for s in range(steps):

@@ -145,6 +145,8 @@ SIGNATURES = {
     "swe_adjoint_backward": [_P, _DP, _DP],
     "swe_adjoint_dt_sequence": [_P, _DP, _DP],
     "swe_adjoint_get_stream": [_P, ctypes.POINTER(_P)],
+    "swe_adjoint_set_boundary": [_P, _I, _I],
+    "swe_adjoint_set_flather_values": [_P, _I, _D, _D],
 }
 _RESTYPES = {"swe_last_error": ctypes.c_char_p}
 

@@ -2,8 +2,8 @@
 
     J = sum over steps, gauges of (b + h - obs)^2
 
-for a ShallowWater-style run (Cartesian, walls) of `steps` self-timed steps
-from still water eta0.  `forward()` runs the step kernels, records the dt
+for a ShallowWater-style run (Cartesian; walls unless `boundaries` says
+otherwise) of `steps` self-timed steps from still water eta0.  `forward()` runs the step kernels, records the dt
 sequence and keeps a checkpoint every `checkpoint_every` steps;
 `backward()` returns dJ/db and dJ/dn over the padded grid from the
 hand-written reverse of every step (swe_adjoint_* in include/swe_b200.h).
@@ -13,12 +13,13 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import LIMITERS, check, dptr
+from ._lib import BC_KIND, LIMITERS, SIDES, check, dptr
 
 
 class MisfitAdjoint:
     def __init__(self, nx, ny, dx, b, eta0, manning=0.025, manning_field=None, gauges=(), steps=1,
-                 checkpoint_every=45, minDepth=1e-3, cfl=0.45, order=2, limiter="mc", coriolis=0.0, dy=None):
+                 checkpoint_every=45, minDepth=1e-3, cfl=0.45, order=2, limiter="mc", coriolis=0.0, dy=None,
+                 boundaries=None):
         lib = _lib.load()
         self._lib = lib
         o = _lib.SweOptions()
@@ -41,6 +42,23 @@ class MisfitAdjoint:
                                      int(checkpoint_every), ctypes.byref(h)))
         self._h = h
         self.set_observations(np.zeros((self.steps, len(g))))
+        for side, bc in (boundaries or {}).items():
+            self.set_boundary(side, bc)
+
+    def set_boundary(self, side, bc):
+        """side: "west", "east", "south" or "north"; bc: "reflect", "outflow",
+        "periodic", or ("flather", eta_ext, u_ext) with a constant exterior
+        state (src/swe.mjs:1026-1126)."""
+        s = SIDES[side]
+        if isinstance(bc, str):
+            if bc not in ("reflect", "outflow", "periodic"):
+                raise ValueError(f"boundary {bc!r}: reflect, outflow, periodic or ('flather', eta, u)")
+            check(self._lib.swe_adjoint_set_boundary(self._h, s, BC_KIND[bc]))
+        else:
+            kind, eta_ext, u_ext = bc
+            if kind != "flather":
+                raise ValueError(f"boundary {bc!r}: reflect, outflow, periodic or ('flather', eta, u)")
+            check(self._lib.swe_adjoint_set_flather_values(self._h, s, float(eta_ext), float(u_ext)))
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

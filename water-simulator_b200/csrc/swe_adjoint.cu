@@ -16,8 +16,9 @@
 // the ghost-cell maps backwards.  The initial depth h = max(0, eta0 - b) is
 // part of the map from b to J.
 //
-// Scope: Cartesian grids, walls (reflect) on every side, any order and
-// limiter, Coriolis, scalar or per-cell Manning n.  No sponge or Flather.
+// Scope: Cartesian grids; per side reflect (the default), outflow, periodic
+// or Flather with a constant exterior state; any order and limiter,
+// Coriolis, scalar or per-cell Manning n.  No sponge or Flather tide.
 #include "../../include/swe_b200.h"
 #include "swe_kernels.cuh"
 #include "swe_split.cuh"
@@ -43,6 +44,9 @@ using swe::StageArgs;
 using swe::pdl_enter;
 
 int fail(int code, const std::string& m) { swe_host::set_error(m); return code; }
+
+// The constant exterior state of the Flather sides (eta, normal velocity).
+struct FlatherValues { double eta[4], u[4]; };
 
 #define CU(call)                                                                      \
   do {                                                                                \
@@ -436,80 +440,88 @@ k_adj_cells_tiled(Geo g, const double* b, const double* h, const double* hu, con
 }
 
 // ---- the rest of the step backwards ----------------------------------------
-// Reflect walls: a ghost takes the clamped mirror source and flips the normal
-// momentum (src/swe.mjs:1026-1039; corners from the S/N pass).  Backwards,
-// each ghost's adjoint moves to its source cell.  Every ghost has exactly one
-// source, and every source is an interior cell, so the map is a gather: one
-// thread per interior cell of the two-cell band along the edges adds the
-// ghosts that map to it, in the order of the forward fill (S/N pass by
-// column then ghost row, south before north; then the W/E pass), and zeroes
-// them.  The sums are therefore the same in every run.
-__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+// The ghost fill backwards.  Every final ghost value is one interior source
+// cell under one map (swe::ghost_source: a copy, a copy with hu or hv
+// negated, or the Flather state of a side, src/swe.mjs:1026-1126), so each
+// ghost's adjoint moves to its source.  The host lists the ghosts of every
+// source in the order of the forward fill; one thread per source adds its
+// ghosts' adjoints in that order and zeroes them, so the sums are the same
+// in every run.  The forward state of the source (the stage input, whose
+// interior the fill left as it was) gives the Flather map's Jacobian.
 
-__device__ __forceinline__ void adj_bc_move(int W, int gi, int gj, int sk, double shu, double shv, double* lb,
-                                            double* lh, double* lhu, double* lhv, double& ab, double& ah,
-                                            double& ahu, double& ahv) {
-  const int gk = (gj + 2) * W + (gi + 2);
-  if (lb) { ab += lb[gk]; lb[gk] = 0; }
-  if (lh) {
-    ah += lh[gk]; lh[gk] = 0;
-    ahu += shu * lhu[gk]; lhu[gk] = 0;
-    ahv += shv * lhv[gk]; lhv[gk] = 0;
+// The Flather ghost backwards (the map of swe::flather_cell): L* is the
+// ghost's adjoint, a* the source's, accumulated.
+__device__ __forceinline__ void flather_rev(int side, double e0, double u0, double minDepth, double eps4, double b,
+                                            double h, double hu, double hv, double Lb, double Lh, double Lhu,
+                                            double Lhv, double& ab, double& ah, double& ahu, double& ahv) {
+  const bool we = side < 2;
+  const double Ln = we ? Lhu : Lhv;                 // the ghost's normal momentum
+  ab += Lb;                                         // g.b = b
+  if (h <= minDepth) {                              // g.h = max(0, e0 - b), momenta 0
+    if (e0 - b > 0) ab -= Lh;
+    return;
   }
-  (void)sk;
+  if (we) ahv += Lhv; else ahu += Lhu;              // the transverse momentum is copied
+  const double qn = we ? hu : hv;
+  const double etaInt = b + h;
+  const double r = sqrt(SWE_G / h);
+  const double sgn = (side == 0 || side == 2) ? 1 : -1;
+  const double uInt = swe::vel(qn, h, eps4);
+  const double Rin = u0 + sgn * e0 * r;
+  const double Rout = uInt - sgn * etaInt * r;
+  const double un = 0.5 * (Rin + Rout);
+  const double en = sgn * (Rin - Rout) / (2 * r);
+  const double gh = swe::jmax0(en - b);
+  // g.h = max(0, en - b), g.qn = g.h un
+  const double Lgh = Lh + Ln * un;
+  const double Lun = Ln * gh;
+  const double Len = en - b > 0 ? Lgh : 0;
+  ab -= Len;
+  // un = (Rin + Rout) / 2, en = sgn (Rin - Rout) / (2 r)
+  const double LRin = 0.5 * Lun + Len * sgn / (2 * r);
+  const double LRout = 0.5 * Lun - Len * sgn / (2 * r);
+  double Lr = -Len * en / r;
+  // Rout = uInt - sgn etaInt r, Rin = u0 + sgn e0 r
+  Lr += -sgn * etaInt * LRout + sgn * e0 * LRin;
+  const double LetaInt = -sgn * r * LRout;
+  ab += LetaInt;
+  ah += LetaInt;
+  double dq, dh;
+  swe::adj::vel_grad(qn, h, eps4, dq, dh);
+  if (we) ahu += LRout * dq; else ahv += LRout * dq;
+  ah += LRout * dh;
+  ah += Lr * (-0.5 * r / h);                        // r = sqrt(G / h)
 }
 
-__global__ void k_adj_bc(int nx, int ny, double* lb, double* lh, double* lhu, double* lhv) {
+// map: sources[nsrc], offsets[nsrc + 1], ghosts[n], transforms[n] (padded
+// cell indices; swe::GT_*).  X: the stage input the fill was applied to.
+__global__ void k_adj_bc(int nsrc, const int* map, const double* b, const double* h, const double* hu,
+                         const double* hv, FlatherValues fv, double minDepth, double eps4, double* lb, double* lh,
+                         double* lhu, double* lhv) {
   pdl_enter();
-  const int W = nx + 4;
-  const int rows[4] = {0, 1, ny - 2, ny - 1};
-  const int cols[4] = {0, 1, nx - 2, nx - 1};
-  const int total = 4 * nx + 4 * ny;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-    int si, sj;
-    if (t < 4 * nx) {                              // the two rows along each of S and N
-      const int r = t / nx;
-      si = t - r * nx;
-      sj = rows[r];
-      if (sj < 0 || sj > ny - 1) continue;
-      bool dup = false;
-      for (int q = 0; q < r; q++) dup |= rows[q] == sj;
-      if (dup) continue;
-    } else {                                       // the two columns along W and E, other rows
-      const int u = t - 4 * nx;
-      sj = u / 4;
-      const int c = u - 4 * sj;
-      si = cols[c];
-      if (si < 0 || si > nx - 1) continue;
-      bool dup = false;
-      for (int q = 0; q < c; q++) dup |= cols[q] == si;
-      for (int q = 0; q < 4; q++) dup |= rows[q] == sj;
-      if (dup) continue;
-    }
-    const int sk = (sj + 2) * W + (si + 2);
-    double ab = lb ? lb[sk] : 0, ah = 0, ahu = 0, ahv = 0;
-    if (lh) { ah = lh[sk]; ahu = lhu[sk]; ahv = lhv[sk]; }
-    // S/N pass: columns i that clamp to si, in increasing order
-    int ilist[5], ni = 0;
-    if (si == 0) { ilist[ni++] = -2; ilist[ni++] = -1; }
-    ilist[ni++] = si;
-    if (si == nx - 1) { ilist[ni++] = nx; ilist[ni++] = nx + 1; }
-    for (int q = 0; q < ni; q++) {
-      const int i = ilist[q];
-      for (int gg = 0; gg < 2; gg++) {
-        if (clampi(gg, 0, ny - 1) == sj)                       // south ghost row -1-gg
-          adj_bc_move(W, i, -1 - gg, sk, 1, -1, lb, lh, lhu, lhv, ab, ah, ahu, ahv);
-        if (clampi(ny - 1 - gg, 0, ny - 1) == sj)              // north ghost row ny+gg
-          adj_bc_move(W, i, ny + gg, sk, 1, -1, lb, lh, lhu, lhv, ab, ah, ahu, ahv);
+  const int* src = map;
+  const int* off = map + nsrc;
+  const int* gcell = off + nsrc + 1;
+  const int* gtr = gcell + off[nsrc];
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < nsrc; u += gridDim.x * blockDim.x) {
+    const int sk = src[u];
+    double ab = lb[sk], ah = lh[sk], ahu = lhu[sk], ahv = lhv[sk];
+    for (int m = off[u]; m < off[u + 1]; m++) {
+      const int gk = gcell[m], tr = gtr[m];
+      const double Lb = lb[gk], Lh = lh[gk], Lhu = lhu[gk], Lhv = lhv[gk];
+      lb[gk] = 0; lh[gk] = 0; lhu[gk] = 0; lhv[gk] = 0;
+      if (tr >= swe::GT_FLATHER) {
+        const int side = tr - swe::GT_FLATHER;
+        flather_rev(side, fv.eta[side], fv.u[side], minDepth, eps4, b[sk], h[sk], hu[sk], hv[sk], Lb, Lh, Lhu,
+                    Lhv, ab, ah, ahu, ahv);
+      } else {
+        ab += Lb;
+        ah += Lh;
+        ahu += tr == swe::GT_FLIPU ? -Lhu : Lhu;
+        ahv += tr == swe::GT_FLIPV ? -Lhv : Lhv;
       }
     }
-    // W/E pass of row sj
-    for (int gg = 0; gg < 2; gg++) {
-      if (clampi(gg, 0, nx - 1) == si) adj_bc_move(W, -1 - gg, sj, sk, -1, 1, lb, lh, lhu, lhv, ab, ah, ahu, ahv);
-      if (clampi(nx - 1 - gg, 0, nx - 1) == si) adj_bc_move(W, nx + gg, sj, sk, -1, 1, lb, lh, lhu, lhv, ab, ah, ahu, ahv);
-    }
-    if (lb) lb[sk] = ab;
-    if (lh) { lh[sk] = ah; lhu[sk] = ahu; lhv[sk] = ahv; }
+    lb[sk] = ab; lh[sk] = ah; lhu[sk] = ahu; lhv[sk] = ahv;
   }
 }
 
@@ -523,7 +535,7 @@ __device__ __forceinline__ void friction_rev(double minDepth, double eps4, doubl
   if (!(n != 0 && n == n)) return;                  // identity (scalar n == 0 skips entirely)
   if (hk <= minDepth) { a1 = 0; a2 = 0; return; }
   const double den = swe::vel_den(hk, eps4);
-  const double u = swe::vel_num(qu, hk) / den, v = swe::vel_num(qv, hk) / den;
+  const double u = swe::qdiv(swe::vel_num(qu, hk), den), v = swe::qdiv(swe::vel_num(qv, hk), den);
   const double speed = hypot(u, v);
   if (speed < 1e-14) return;
   const double P = pow(hk, 4.0 / 3.0);
@@ -630,9 +642,12 @@ __global__ void k_adj_misfit(const double* b, const double* h, const int* gcell,
     lb[k] = ab;
   }
 }
-__global__ void k_set_dt(Control* ctl, const double* dts, int s) {
+__global__ void k_set_dt(Control* ctl, const double* dts, int s, FlatherValues fv) {
   pdl_enter();
-  if (threadIdx.x == 0) { ctl->dt = dts[s]; ctl->stop = 0; }
+  if (threadIdx.x == 0) {
+    ctl->dt = dts[s]; ctl->stop = 0;
+    for (int q = 0; q < 4; q++) { ctl->fl_eta[q] = fv.eta[q]; ctl->fl_u[q] = fv.u[q]; }
+  }
 }
 __global__ void k_record_dt(const Control* ctl, double* dts, int s) {
   pdl_enter();
@@ -690,6 +705,10 @@ struct swe_adjoint {
   bool forward_done = false;
   bool pdl = true;                 // programmatic dependent launch between the stepping kernels
   bool fixed_dt = false;         // forward uses the given dt sequence instead of maxDt()
+  int kind[4] = {SWE_BC_REFLECT, SWE_BC_REFLECT, SWE_BC_REFLECT, SWE_BC_REFLECT};   // W, E, S, N
+  FlatherValues flv = {};        // exterior state of the Flather sides
+  int* gmap = nullptr;           // the ghost fill by source (k_adj_bc)
+  int nsrc = 0;
   std::vector<double> dts_host;  // the dt sequence, read once per backward pass
 };
 
@@ -729,7 +748,7 @@ StageArgs stage_args(const swe_adjoint* s, double* const* in, double* const* out
 BCArgs bc_args(const swe_adjoint* s, double* const* f) {
   BCArgs a;
   a.nx = s->o.nx; a.ny = s->o.ny; a.W = s->W; a.H = s->H;
-  for (int q = 0; q < 4; q++) a.kind[q] = SWE_BC_REFLECT;
+  for (int q = 0; q < 4; q++) a.kind[q] = s->kind[q];
   a.minDepth = s->o.min_depth; a.eps4 = s->eps4;
   a.b = s->b; a.h = f[0]; a.hu = f[1]; a.hv = f[2];
   return a;
@@ -737,7 +756,7 @@ BCArgs bc_args(const swe_adjoint* s, double* const* f) {
 
 int G1(const swe_adjoint* s) { return std::min(4096, (s->N + 255) / 256); }
 int bcb(const swe_adjoint* s) { return (4 * s->o.ny + 4 * (s->o.nx + 4) + 255) / 256; }
-int adjbc_blocks(const swe_adjoint* s) { return (4 * s->o.nx + 4 * s->o.ny + 255) / 256; }
+int adjbc_blocks(const swe_adjoint* s) { return std::max(1, (s->nsrc + 255) / 256); }
 
 // A launch on the handle's stream that, with `pdl`, may be scheduled while
 // the previous kernel drains (every kernel here waits for its predecessors
@@ -772,9 +791,10 @@ int fwd_step(swe_adjoint* s, double* const* X, bool auto_dt, int step_index) {
     swe::PrepArgs p;
     std::memset(&p, 0, sizeof p);
     p.mode = 1; p.cfl = s->o.cfl; p.t_end = INFINITY;
+    for (int q = 0; q < 4; q++) { p.fl_eta[q] = s->flv.eta[q]; p.fl_u[q] = s->flv.u[q]; }
     LAUNCH(swe::k_prepare, dim3(1), dim3(32), s->ctl, p);
   } else {
-    LAUNCH(k_set_dt, dim3(1), dim3(32), s->ctl, (const double*)s->dts, step_index);
+    LAUNCH(k_set_dt, dim3(1), dim3(32), s->ctl, (const double*)s->dts, step_index, s->flv);
   }
   const dim3 spb(swe::SP_THREADS);
   const int nparts = (int)(s->sgrid.x * s->sgrid.y);
@@ -867,7 +887,7 @@ swe::SplitBufs tape_bufs(const swe_adjoint* s, const Inter& it) {
 int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
   const dim3 spb(swe::SP_THREADS);
   const int nparts = (int)(s->sgrid.x * s->sgrid.y);
-  LAUNCH(k_set_dt, dim3(1), dim3(32), s->ctl, (const double*)s->dts, k);
+  LAUNCH(k_set_dt, dim3(1), dim3(32), s->ctl, (const double*)s->dts, k, s->flv);
   // the step input with its ghosts, in X (U0 of the in-place stage 2) and on the tape
   LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, X), (const Control*)s->ctl, 0);
   if (int rc = copy3(s, T.W1, X)) return rc;
@@ -905,15 +925,73 @@ int reverse_step(swe_adjoint* s, int k, const Tape& T) {
          s->ab.lR[2]);
   int rc = residual_adjoint(s, T.Bp, T.it2, T.th2, dt, lB);
   if (rc) return rc;
-  LAUNCH(k_adj_bc, dim3(adjbc_blocks(s)), dim3(256), s->o.nx, s->o.ny, s->lb, lB[0], lB[1], lB[2]);
+  LAUNCH(k_adj_bc, dim3(adjbc_blocks(s)), dim3(256), s->nsrc, (const int*)s->gmap, (const double*)s->b,
+         (const double*)T.Bp[0], (const double*)T.Bp[1], (const double*)T.Bp[2], s->flv, s->o.min_depth, s->eps4,
+         s->lb, lB[0], lB[1], lB[2]);
   // dryClean and B = W1 + dt R1 backwards: lW1 += lB, lR1 = dt lB
   LAUNCH(k_adj_tail1, dim3(gb), dim3(256), s->W, s->H, s->o.min_depth, dt, (const double*)T.hB,
          (const double*)lB[0], (const double*)lB[1], (const double*)lB[2], lA[0], lA[1], lA[2], s->ab.lR[0],
          s->ab.lR[1], s->ab.lR[2]);
   rc = residual_adjoint(s, T.W1, T.it1, T.th1, dt, lA);
   if (rc) return rc;
-  LAUNCH(k_adj_bc, dim3(adjbc_blocks(s)), dim3(256), s->o.nx, s->o.ny, s->lb, lA[0], lA[1], lA[2]);
+  LAUNCH(k_adj_bc, dim3(adjbc_blocks(s)), dim3(256), s->nsrc, (const int*)s->gmap, (const double*)s->b,
+         (const double*)T.W1[0], (const double*)T.W1[1], (const double*)T.W1[2], s->flv, s->o.min_depth, s->eps4,
+         s->lb, lA[0], lA[1], lA[2]);
   CU(cudaGetLastError());
+  return SWE_OK;
+}
+
+// The ghost fill by source, for k_adj_bc: every ghost in the order of the
+// forward fill (swe::apply_bc_range: the W/E rings row by row, then the S/N
+// rings column by column), grouped by source in order of first appearance.
+int build_ghost_map(swe_adjoint* s) {
+  const int nx = s->o.nx, ny = s->o.ny, W = s->W;
+  const int nwe = 4 * ny, nsn = 4 * (nx + 4);
+  std::vector<int> src;
+  std::vector<std::vector<std::pair<int, int>>> members;
+  std::unordered_map<int, int> group;
+  for (int q = 0; q < nwe + nsn; q++) {
+    int i, j;
+    if (q < nwe) {
+      j = q / 4;
+      const int r = q % 4;
+      i = r < 2 ? -1 - r : nx + (r - 2);
+    } else {
+      const int p = q - nwe;
+      i = p / 4 - 2;
+      const int r = p % 4;
+      j = r < 2 ? -1 - r : ny + (r - 2);
+    }
+    int si, sj;
+    const int tr = swe::ghost_source(s->kind, nx, ny, i, j, si, sj);
+    const int gk = (j + 2) * W + (i + 2), sk = (sj + 2) * W + (si + 2);
+    auto it = group.find(sk);
+    int u;
+    if (it == group.end()) {
+      u = (int)src.size();
+      group.emplace(sk, u);
+      src.push_back(sk);
+      members.emplace_back();
+    } else {
+      u = it->second;
+    }
+    members[u].push_back({gk, tr});
+  }
+  std::vector<int> map(src);
+  map.push_back(0);
+  for (auto& m : members) map.push_back(map.back() + (int)m.size());
+  for (auto& m : members)
+    for (auto& e : m) map.push_back(e.first);
+  for (auto& m : members)
+    for (auto& e : m) map.push_back(e.second);
+  CU(cudaStreamSynchronize(s->st));
+  if (s->gmap) cudaFree(s->gmap);
+  s->gmap = nullptr;
+  s->nsrc = 0;
+  CU(cudaMalloc(&s->gmap, sizeof(int) * map.size()));
+  CU(cudaMemcpyAsync(s->gmap, map.data(), sizeof(int) * map.size(), cudaMemcpyHostToDevice, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  s->nsrc = (int)src.size();
   return SWE_OK;
 }
 
@@ -921,6 +999,7 @@ void free_adj(swe_adjoint* s) {
   for (double* p : s->allocs) cudaFree(p);
   if (s->gk) cudaFree(s->gk);
   if (s->gmeta) cudaFree(s->gmeta);
+  if (s->gmap) cudaFree(s->gmap);
   if (s->ctl) cudaFree(s->ctl);
   if (s->st) cudaStreamDestroy(s->st);
 }
@@ -1040,6 +1119,7 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
     if (cudaStreamSynchronize(s->st) != cudaSuccess) return bail(fail(SWE_ECUDA, "swe_adjoint_create: upload"));
   }
   if (cudaStreamSynchronize(s->st) != cudaSuccess) return bail(fail(SWE_ECUDA, "swe_adjoint_create: upload"));
+  if (int rc = build_ghost_map(s)) return bail(rc);
   *out = s;
   return SWE_OK;
 }
@@ -1148,6 +1228,25 @@ int swe_adjoint_dt_sequence(swe_adjoint* s, double* dts_out, const double* dts_i
   if (dts_out) CU(cudaMemcpyAsync(dts_out, s->dts, sizeof(double) * s->steps, cudaMemcpyDeviceToHost, s->st));
   CU(cudaStreamSynchronize(s->st));
   return SWE_OK;
+}
+
+int swe_adjoint_set_boundary(swe_adjoint* s, int side, int kind) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (side < 0 || side > 3 || kind < SWE_BC_REFLECT || kind > SWE_BC_FLATHER)
+    return fail(SWE_EINVAL, "swe_adjoint_set_boundary: side 0..3 (W, E, S, N), kind reflect/outflow/periodic/flather");
+  s->kind[side] = kind;
+  s->forward_done = false;
+  return build_ghost_map(s);
+}
+
+int swe_adjoint_set_flather_values(swe_adjoint* s, int side, double eta_ext, double u_ext) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (side < 0 || side > 3) return fail(SWE_EINVAL, "swe_adjoint_set_flather_values: side 0..3 (W, E, S, N)");
+  s->flv.eta[side] = eta_ext;
+  s->flv.u[side] = u_ext;
+  s->kind[side] = SWE_BC_FLATHER;
+  s->forward_done = false;
+  return build_ghost_map(s);
 }
 
 int swe_adjoint_get_stream(swe_adjoint* s, void** stream) {

@@ -224,40 +224,54 @@ __device__ __forceinline__ Cell flather_cell(const BCArgs& a, const Control* ctl
   return g;
 }
 
-// Final value of a W/E ghost (i < 0 or i >= nx) in interior row j.
-__device__ Cell we_ghost(const BCArgs& a, const Control* ctl, int i, int j) {
+// Every final ghost value is one interior cell under one map (the ghost's
+// source and transform): a copy, a copy with the x or the y momentum negated
+// (reflect W/E, S/N), or the Flather state of one side.  ghost_source gives
+// both for the ghost (i, j) -- W/E ghosts (i < 0 or i >= nx) of interior rows,
+// S/N ghosts (j < 0 or j >= ny) of columns [-2, nx+2) -- for the forward fill
+// here and for the adjoint's reverse of it.
+enum { GT_COPY = 0, GT_FLIPU = 1, GT_FLIPV = 2, GT_FLATHER = 4 };   // GT_FLATHER + side
+__host__ __device__ __forceinline__ int clampi_hd(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+__host__ __device__ __forceinline__ int modi_hd(int v, int n) { int r = v % n; return r < 0 ? r + n : r; }
+
+__host__ __device__ __forceinline__ int we_source(const int* kind, int nx, int i, int j, int& si, int& sj) {
   const int side = i < 0 ? 0 : 1;
-  const int kind = a.kind[side];
-  if (kind == BC_REFLECT) {
-    int si = side == 0 ? -1 - i : 2 * a.nx - 1 - i;
-    si = clampi(si, 0, a.nx - 1);
-    Cell s = load_cell(a, si, j);
-    Cell g; g.b = s.b; g.h = s.h; g.hu = -s.hu; g.hv = s.hv;
-    return g;
+  sj = j;
+  switch (kind[side]) {
+    case BC_REFLECT: si = clampi_hd(side == 0 ? -1 - i : 2 * nx - 1 - i, 0, nx - 1); return GT_FLIPU;
+    case BC_OUTFLOW: si = clampi_hd(i, 0, nx - 1); return GT_COPY;
+    case BC_PERIODIC: si = modi_hd(i, nx); return GT_COPY;
+    default: si = clampi_hd(i, 0, nx - 1); return GT_FLATHER + side;
   }
-  if (kind == BC_OUTFLOW) return load_cell(a, clampi(i, 0, a.nx - 1), j);
-  if (kind == BC_PERIODIC) return load_cell(a, modi(i, a.nx), j);
-  return flather_cell(a, ctl, side, load_cell(a, clampi(i, 0, a.nx - 1), j));
+}
+__host__ __device__ __forceinline__ int ghost_source(const int* kind, int nx, int ny, int i, int j, int& si,
+                                                     int& sj) {
+  if (j >= 0 && j < ny) return we_source(kind, nx, i, j, si, sj);
+  const int side = j < 0 ? 2 : 3;
+  switch (kind[side]) {
+    case BC_REFLECT:
+      si = clampi_hd(i, 0, nx - 1);
+      sj = clampi_hd(side == 2 ? -1 - j : 2 * ny - 1 - j, 0, ny - 1);
+      return GT_FLIPV;
+    case BC_OUTFLOW: si = clampi_hd(i, 0, nx - 1); sj = clampi_hd(j, 0, ny - 1); return GT_COPY;
+    case BC_PERIODIC: {
+      const int pj = modi_hd(j, ny);
+      if (i >= 0 && i < nx) { si = i; sj = pj; return GT_COPY; }
+      return we_source(kind, nx, i, pj, si, sj);      // the W/E ghost of row pj, recomputed
+    }
+    default: si = clampi_hd(i, 0, nx - 1); sj = clampi_hd(j, 0, ny - 1); return GT_FLATHER + side;
+  }
 }
 
-// Final value of a S/N ghost (j < 0 or j >= ny), i in [-2, nx+2).
-__device__ Cell sn_ghost(const BCArgs& a, const Control* ctl, int i, int j) {
-  const int side = j < 0 ? 2 : 3;
-  const int kind = a.kind[side];
-  if (kind == BC_REFLECT) {
-    int sj = side == 2 ? -1 - j : 2 * a.ny - 1 - j;
-    sj = clampi(sj, 0, a.ny - 1);
-    Cell s = load_cell(a, clampi(i, 0, a.nx - 1), sj);
-    Cell g; g.b = s.b; g.h = s.h; g.hu = s.hu; g.hv = -s.hv;
-    return g;
-  }
-  if (kind == BC_OUTFLOW) return load_cell(a, clampi(i, 0, a.nx - 1), clampi(j, 0, a.ny - 1));
-  if (kind == BC_PERIODIC) {
-    const int sj = modi(j, a.ny);
-    if (i >= 0 && i < a.nx) return load_cell(a, i, sj);
-    return we_ghost(a, ctl, i, sj);
-  }
-  return flather_cell(a, ctl, side, load_cell(a, clampi(i, 0, a.nx - 1), clampi(j, 0, a.ny - 1)));
+// Final value of the ghost (i, j).
+__device__ __forceinline__ Cell ghost_cell(const BCArgs& a, const Control* ctl, int i, int j) {
+  int si, sj;
+  const int tr = ghost_source(a.kind, a.nx, a.ny, i, j, si, sj);
+  Cell c = load_cell(a, si, sj);
+  if (tr >= GT_FLATHER) return flather_cell(a, ctl, tr - GT_FLATHER, c);
+  if (tr == GT_FLIPU) c.hu = -c.hu;
+  else if (tr == GT_FLIPV) c.hv = -c.hv;
+  return c;
 }
 
 // Ghost cells q0, q0 + stride, ... of one grid.
@@ -271,14 +285,13 @@ __device__ __forceinline__ void apply_bc_range(const BCArgs& a, const Control* c
       j = q / 4;
       const int r = q % 4;                  // 0,1 west rings; 2,3 east rings
       i = r < 2 ? -1 - r : a.nx + (r - 2);
-      c = we_ghost(a, ctl, i, j);
     } else {
       const int p = q - nwe;
       i = p / 4 - 2;
       const int r = p % 4;
       j = r < 2 ? -1 - r : a.ny + (r - 2);
-      c = sn_ghost(a, ctl, i, j);
     }
+    c = ghost_cell(a, ctl, i, j);
     const int k = (j + 2) * a.W + (i + 2);
     a.b[k] = c.b; a.h[k] = c.h; a.hu[k] = c.hu; a.hv[k] = c.hv;
   }
@@ -401,8 +414,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, Control* ctl, int
       V_c = vel_num(hv_c, h_c);
     } else {
       const double den = vel_den(h_c, eps4);
-      U_c = vel_num(hu_c, h_c) / den;
-      V_c = vel_num(hv_c, h_c) / den;
+      U_c = qdiv(vel_num(hu_c, h_c), den);
+      V_c = qdiv(vel_num(hv_c, h_c), den);
     }
     const int sr = (r + 4) & 3;     // ring slot of row r (r >= -3)
     s_b[sr][c] = b_c; s_h[sr][c] = h_c; s_U[sr][c] = U_c; s_V[sr][c] = V_c;
@@ -584,12 +597,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, Control* ctl, int
             if (nh <= dry) { nhu = 0; nhv = 0; }
             else if (n != 0 && n == n) {
               const double den = vel_den(nh, eps4);
-              const double u = vel_num(nhu, nh) / den, v = vel_num(nhv, nh) / den;
+              const double u = qdiv(vel_num(nhu, nh), den), v = qdiv(vel_num(nhv, nh), den);
               const double speed = hypot(u, v);
               if (!(speed < 1e-14)) {
                 const double denom = 1 + dt * SWE_G * n * n * speed / pow(nh, 4.0 / 3.0);
-                nhu = nhu / denom;
-                nhv = nhv / denom;
+                nhu = qdiv(nhu, denom);
+                nhv = qdiv(nhv, denom);
               }
             }
           }
@@ -611,7 +624,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, Control* ctl, int
           if (!(nh <= dry)) {
             const double cc = sqrt(SWE_G * nh);
             const double den = vel_den(nh, eps4);
-            const double u = fabs(vel_num(nhu, nh) / den), v = fabs(vel_num(nhv, nh) / den);
+            const double u = fabs(qdiv(vel_num(nhu, nh), den)), v = fabs(qdiv(vel_num(nhv, nh), den));
             const double sr5 = (u + cc) / s_m[M_DX][m3] + (v + cc) / s_m[M_CFL][m3];
             if (sr5 > locMax) locMax = sr5;
           }

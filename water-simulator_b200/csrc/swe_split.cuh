@@ -290,7 +290,7 @@ __device__ __forceinline__ void split_faces_finish_l(const StageArgs& a, const S
       U = vel_num(hu, h); V = vel_num(hv, h);
     } else {
       const double den = vel_den(h, eps4);
-      U = vel_num(hu, h) / den; V = vel_num(hv, h) / den;
+      U = qdiv(vel_num(hu, h), den); V = qdiv(vel_num(hv, h), den);
     }
     sm.U[ly][c] = U; sm.V[ly][c] = V;
   }
@@ -633,12 +633,12 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
         if (nh <= dry) { nhu = 0; nhv = 0; }
         else if (n != 0 && n == n) {
           const double den = vel_den(nh, eps4);
-          const double u = vel_num(nhu, nh) / den, v = vel_num(nhv, nh) / den;
+          const double u = qdiv(vel_num(nhu, nh), den), v = qdiv(vel_num(nhv, nh), den);
           const double speed = hypot(u, v);
           if (!(speed < 1e-14)) {
             const double denom = 1 + dt * SWE_G * n * n * speed / pow(nh, 4.0 / 3.0);
-            nhu = nhu / denom;
-            nhv = nhv / denom;
+            nhu = qdiv(nhu, denom);
+            nhv = qdiv(nhv, denom);
           }
         }
       }
@@ -660,7 +660,7 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
       if (!(nh <= dry)) {
         const double cc = sqrt(SWE_G * nh);
         const double den = vel_den(nh, eps4);
-        const double u = fabs(vel_num(nhu, nh) / den), v = fabs(vel_num(nhv, nh) / den);
+        const double u = fabs(qdiv(vel_num(nhu, nh), den)), v = fabs(qdiv(vel_num(nhv, nh), den));
         const double sr5 = (u + cc) / dxr + (v + cc) / a.m.dyCFL[gj];
         if (sr5 > locMax) locMax = sr5;
       }
