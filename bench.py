@@ -288,12 +288,34 @@ def all_wet_summary(torch, swe, steps, device=0, warm=32):
             "value": n * n * steps / (ms / 1e3), "unit": UNIT, "steps": steps, "ms_per_step": ms / steps,
             "dry_cells_after": dry,
             "step_phase_ms": dict(zip(["prepare", "bc1", "stage1", "bc2", "stage2"], avg)),
-            "roofline": {"bound": "hbm", "limiter": "FP64 issue latency (see fp64 below)",
+            "roofline": {"bound": "hbm", "limiter": "the FP64 pipe (fp64_ceiling)",
                          "achieved": st2, "peak": peak, "unit": "GB/s", "frac": st2 / peak,
                          "peak_source": kind, "algorithmic_bytes_per_launch": STAGE_BYTES["stage2"] * n * n,
-                         "traffic": profile_figure("k_split_faces_allwet2048.md", "dram_bytes_per_stage2_pair:"),
-                         "fp64_pipe_frac": profile_figure("k_split_faces_allwet2048.md", "fp64_pipe_active_frac:")},
+                         "traffic": profile_figure(ALLWET_PROFILE, "dram_bytes_per_stage2_pair:")},
+            "fp64_ceiling": fp64_ceiling(n * n * steps / (ms / 1e3), peak),
             "clocks": clocks}
+
+
+ALLWET_PROFILE = "k_split_faces_allwet2048.md"
+
+
+def fp64_ceiling(cups, peak):
+    """What the FP64 pipe allows on the all-wet grid, from the committed ncu
+    capture of the stage-2 pair: each kernel's duration times the share of
+    it the FP64 pipe was busy is the time its FP64 work needs at full pipe
+    rate; the rate with every stage at that bound, against the rate that 60%
+    of HBM bandwidth would give at 136 B per cell-update."""
+    f = {k: profile_figure(ALLWET_PROFILE, k + ":") for k in
+         ("fp64_pipe_active_frac_faces", "fp64_pipe_active_frac_cells", "ncu_us_faces", "ncu_us_cells")}
+    if any(v is None for v in f.values()):
+        return None
+    pair = f["ncu_us_faces"] + f["ncu_us_cells"]
+    floor = f["fp64_pipe_active_frac_faces"] * f["ncu_us_faces"] + f["fp64_pipe_active_frac_cells"] * f["ncu_us_cells"]
+    return {"fp64_pipe_active_frac": {"faces": f["fp64_pipe_active_frac_faces"], "cells": f["fp64_pipe_active_frac_cells"]},
+            "stage2_pair_us": pair, "stage2_fp64_bound_us": floor,
+            "cups_at_fp64_bound": cups * pair / floor,
+            "cups_at_60pct_hbm": 0.6 * peak * 1e9 / (STAGE_BYTES["stage1"] + STAGE_BYTES["stage2"]),
+            "source": "profiles/" + ALLWET_PROFILE}
 
 
 def ensemble_summary(torch, swe, steps=200, fused_steps=50, device=0):

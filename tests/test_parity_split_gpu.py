@@ -100,11 +100,13 @@ def test_dry_tile_flags_follow_host_writes(swe, monkeypatch):
 
 @pytest.mark.parametrize("nx,ny", [(256, 96), (255, 97), (30, 9)])
 def test_tensor_map_tile_copies_give_the_same_bits(swe, monkeypatch, nx, ny):
-    """The face kernel's state tile fetched by tensor-map copies (even padded
-    width) against the per-element copies (SWE_B200_TMA=0): the same bits
-    after 150 steps of a flooding beach with friction, tiles at every edge of
-    the grid included (the copies fill outside the grid with zeros).  An odd
-    padded width always takes the per-element copies."""
+    """The face kernel's state tile and the cell kernel's face and depth
+    tiles fetched by tensor-map copies (even padded width) against the
+    per-element loads (SWE_B200_TMA=0): the same bits after 150 steps of a
+    flooding beach with friction, tiles at every edge of the grid and tiles
+    beside dry ones included (the copies fill outside the grid with zeros,
+    and faces of dry tiles are read as +0 either way).  An odd padded width
+    always takes the per-element loads."""
     import numpy as np
     from water_simulator_b200 import workloads
 

@@ -108,7 +108,7 @@ __device__ __forceinline__ FaceAdj xface_adj(const Geo& g, const Inter& it, cons
   f.lpR = inv * a.lR[1][kR];
   const double linv = M * (a.lR[0][kR] - a.lR[0][kL]) + NpR * a.lR[1][kR] - NpL * a.lR[1][kL] +
                       T * (a.lR[2][kR] - a.lR[2][kL]);
-  f.lth = linv / g.dxRow[j];
+  f.lth = swe::qdiv(linv, g.dxRow[j]);          // adjoints are often +-0 (qdiv)
   return f;
 }
 
@@ -128,7 +128,7 @@ __device__ __forceinline__ FaceAdj yface_adj(const Geo& g, const Inter& it, cons
   f.lpR = invR * a.lR[2][kR];
   const double linvL = -(M * a.lR[0][kL] + NpL * a.lR[2][kL] + T * a.lR[1][kL]);
   const double linvR = M * a.lR[0][kR] + NpR * a.lR[2][kR] + T * a.lR[1][kR];
-  f.lth = linvL / g.dyRowN[j] + linvR / g.dyRowS[j + 1];
+  f.lth = swe::qdiv(linvL, g.dyRowN[j]) + swe::qdiv(linvR, g.dyRowS[j + 1]);
   return f;
 }
 
@@ -213,8 +213,8 @@ k_adj_xfaces(Geo g, const double* b, const double* h, Inter it, const double* th
     const FaceAdj f = xface_adj(g, it, theta, a, k, i, j);
     double lM = f.lM;
     const double M = it.fx[F_M][k];
-    if (M > 0) lM += lout_of(g, it, theta, h, dt, a, k) / g.dxRow[j];
-    if (M < 0) lM -= lout_of(g, it, theta, h, dt, a, k + 1) / g.dxRow[j];
+    if (M > 0) lM += swe::qdiv(lout_of(g, it, theta, h, dt, a, k), g.dxRow[j]);
+    if (M < 0) lM -= swe::qdiv(lout_of(g, it, theta, h, dt, a, k + 1), g.dxRow[j]);
     gx = swe::adj::face_rev(xface_in(g, b, h, it, k), g.minDepth, lM, f.lN, f.lT, f.lpL, f.lpR);
   }
   const double* p = &gx.bL;
@@ -243,8 +243,8 @@ k_adj_yfaces(Geo g, const double* b, const double* h, Inter it, const double* th
     const FaceAdj f = yface_adj(g, it, theta, a, k, i, j);
     double lM = f.lM;
     const double M = it.fy[F_M][k];
-    if (M > 0) lM += lout_of(g, it, theta, h, dt, a, k) / g.dyRowN[j];
-    if (M < 0) lM -= lout_of(g, it, theta, h, dt, a, k + g.W) / g.dyRowS[j + 1];
+    if (M > 0) lM += swe::qdiv(lout_of(g, it, theta, h, dt, a, k), g.dyRowN[j]);
+    if (M < 0) lM -= swe::qdiv(lout_of(g, it, theta, h, dt, a, k + g.W), g.dyRowS[j + 1]);
     gy = swe::adj::face_rev(yface_in(g, b, h, it, k), g.minDepth, lM, f.lN, f.lT, f.lpL, f.lpR);
   }
   const double* p = &gy.bL;
@@ -302,8 +302,8 @@ __device__ __forceinline__ void bed_term_adj(const Geo& g, const double* b, cons
   const double hP = swe::jmax0(aP), hM = swe::jmax0(aM);
   const double div = d == 0 ? g.dxRow[j] : g.bedPhi[j];
   const double lterm = a.lR[1 + d][k];
-  const double lhPM = lterm * (-SWE_G * 0.5 * sB / div);
-  const double ldb = lterm * (-SWE_G * 0.5 * (hP + hM)) / div;
+  const double lhPM = lterm * swe::qdiv(-SWE_G * 0.5 * sB, div);
+  const double ldb = swe::qdiv(lterm * (-SWE_G * 0.5 * (hP + hM)), div);
   double leC = 0;
   if (aP > 0) { leC += lhPM; ls[0] += 0.5 * lhPM; db -= lhPM; ls[1] -= 0.5 * lhPM; }
   if (aM > 0) { leC += lhPM; ls[0] -= 0.5 * lhPM; db -= lhPM; ls[1] += 0.5 * lhPM; }
@@ -538,12 +538,12 @@ __device__ __forceinline__ void friction_rev(double minDepth, double eps4, doubl
   const double u = swe::qdiv(swe::vel_num(qu, hk), den), v = swe::qdiv(swe::vel_num(qv, hk), den);
   const double speed = hypot(u, v);
   if (speed < 1e-14) return;
-  const double P = pow(hk, 4.0 / 3.0);
+  const double P = swe::pow43(hk);                // the forward's own value
   const double K = dt * SWE_G * n * n;
   const double denom = 1 + K * speed / P;
   const double ghu = a1, ghv = a2;
-  const double lden = -(ghu * qu + ghv * qv) / (denom * denom);
-  double gh = 0, gq = ghu / denom, gr = ghv / denom;
+  const double lden = swe::qdiv(-(ghu * qu + ghv * qv), denom * denom);
+  double gh = 0, gq = swe::qdiv(ghu, denom), gr = swe::qdiv(ghv, denom);
   const double lspeed = lden * K / P;
   const double lP = -lden * K * speed / (P * P);
   if (ln) ln[k] += lden * dt * SWE_G * 2 * n * speed / P;

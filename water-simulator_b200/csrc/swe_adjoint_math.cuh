@@ -47,7 +47,7 @@ __device__ __forceinline__ void vel_grad(double q, double h, double eps4, double
   const double sD = sqrt(D);
   const double dD = 4 * h * h * h * (big ? 2 : 1);
   dq = SWE_SQRT2 * h / sD;
-  dh = SWE_SQRT2 * q / sD - 0.5 * SWE_SQRT2 * h * q * dD / (D * sD);
+  dh = qdiv(SWE_SQRT2 * q, sD) - qdiv(0.5 * SWE_SQRT2 * h * q * dD, D * sD);   // q is often +-0
 }
 
 // Reverse of hllc(): given the output adjoints (gM, gN, gT), add the
@@ -62,8 +62,8 @@ __device__ __forceinline__ void hllc_rev(double hL, double huL, double hvL, doub
   // division.  v only scales the transverse flux, so a reciprocal (reused
   // by the reverse of u = hu / h at the end) serves.
   const double rL = wetL ? 1 / hL : 0, rR = wetR ? 1 / hR : 0;
-  const double uL = wetL ? huL / hL : 0, vL = wetL ? hvL * rL : 0;
-  const double uR = wetR ? huR / hR : 0, vR = wetR ? hvR * rR : 0;
+  const double uL = wetL ? qdiv(huL, hL) : 0, vL = wetL ? hvL * rL : 0;
+  const double uR = wetR ? qdiv(huR, hR) : 0, vR = wetR ? hvR * rR : 0;
   const double cL = sqrt(SWE_G * jmax(hL, 0)), cR = sqrt(SWE_G * jmax(hR, 0));
   double sL, sR, a = 0, hStar = 0, qL = 1, qR = 1;
   int speeds;                                       // 0 dry|wet, 1 wet|dry, 2 wet|wet
@@ -92,7 +92,7 @@ __device__ __forceinline__ void hllc_rev(double hL, double huL, double hvL, doub
   } else {
     const double num = sL * hR * (uR - sR) - sR * hL * (uL - sL);
     const double den = hR * (uR - sR) - hL * (uL - sL);
-    const double sM = fabs(den) > 1e-30 ? num / den : 0.5 * (sL + sR);
+    const double sM = fabs(den) > 1e-30 ? qdiv(num, den) : 0.5 * (sL + sR);
     const bool takeL = sM >= 0;
     const double FL0 = huL, FL1 = huL * uL + 0.5 * SWE_G * hL * hL;
     const double FR0 = huR, FR1 = huR * uR + 0.5 * SWE_G * hR * hR;

@@ -99,6 +99,8 @@ struct swe_sim {
   int* d_odry[2] = {nullptr, nullptr};             // per tile of A / B: all h == 0 (swe_split.cuh)
   swe::TileMaps tmaps[2];                          // the face kernel's tensor maps over A and B
   int tma = 0;                                     // 1: they are in use
+  swe::CellMaps cmaps[2];                          // the cell kernel's, per stage
+  int cell_tma = 0;                                // 1: they are in use
   swe::SplitBufs sb;
   dim3 sgrid;
   // Whether the tiled cell kernels may settle dry tiles (swe_split.cuh).
@@ -322,32 +324,69 @@ int launch_bc(swe_sim* s, double* const* f, int respect_stop, bool pdl = false) 
 // W x H array of doubles, box SSXT x SSY, zeros outside.  A row stride that
 // is not a multiple of 16 bytes (odd W), a driver without the encoder, or
 // SWE_B200_TMA=0 leaves the per-element copies in use (the same bits).
-void make_tile_maps(swe_sim* s) {
-  s->tma = 0;
-  const char* env = std::getenv("SWE_B200_TMA");
-  if (env && std::strcmp(env, "0") == 0) return;
-  if ((sizeof(double) * (size_t)s->W) % 16 != 0) return;
+// The driver's tensor-map encoder, or null; and whether the tile copies are
+// on for this grid (SWE_B200_TMA=0 turns them off; a row stride that is not
+// a multiple of 16 bytes cannot take them).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
         q != cudaDriverEntryPointSuccess || !fn)
-      return;
+      return nullptr;
     encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
+  return encode;
+}
+bool tma_wanted(const swe_sim* s) {
+  const char* env = std::getenv("SWE_B200_TMA");
+  if (env && std::strcmp(env, "0") == 0) return false;
+  return (sizeof(double) * (size_t)s->W) % 16 == 0;
+}
+// A 2-D map over one W x H field of doubles with the given box.
+bool encode_field(PFN_cuTensorMapEncodeTiled_v12000 encode, const swe_sim* s, CUtensorMap* m, double* base,
+                  int bx, int by) {
   const cuuint64_t dims[2] = {(cuuint64_t)s->W, (cuuint64_t)s->H};
   const cuuint64_t strides[1] = {(cuuint64_t)s->W * sizeof(double)};
-  const cuuint32_t box[2] = {(cuuint32_t)swe::SSXT, (cuuint32_t)swe::SSY};
+  const cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
   const cuuint32_t estr[2] = {1, 1};
+  return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The cell kernel's maps: the face fields (one set of buffers for both
+// stages) and the stage input's depth.
+void make_cell_maps(swe_sim* s) {
+  s->cell_tma = 0;
+  if (!s->d_split || !tma_wanted(s)) return;
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return;
+  using swe::SPX;
+  using swe::SPY;
+  for (int st = 0; st < 2; st++) {
+    swe::CellMaps& c = s->cmaps[st];
+    bool ok = encode_field(encode, s, &c.m[swe::CM_XM], s->sb.fx[swe::F_M], SPX + 4, SPY + 2) &&
+              encode_field(encode, s, &c.m[swe::CM_YM], s->sb.fy[swe::F_M], SPX + 4, SPY + 3) &&
+              encode_field(encode, s, &c.m[swe::CM_H], st == 0 ? s->d_A[0] : s->d_B[0], SPX + 4, SPY + 2);
+    for (int q = 0; q < 3 && ok; q++)
+      ok = encode_field(encode, s, &c.m[swe::CM_XT + q], s->sb.fx[q + 1], SPX + 2, SPY) &&
+           encode_field(encode, s, &c.m[swe::CM_YT + q], s->sb.fy[q + 1], SPX, SPY + 1);
+    if (!ok) return;
+  }
+  s->cell_tma = 1;
+}
+
+void make_tile_maps(swe_sim* s) {
+  s->tma = 0;
+  if (!tma_wanted(s)) return;
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return;
   double* src[2][4] = {{s->d_b, s->d_A[0], s->d_A[1], s->d_A[2]}, {s->d_b, s->d_B[0], s->d_B[1], s->d_B[2]}};
   for (int st = 0; st < 2; st++)
-    for (int f = 0; f < 4; f++) {
-      const CUresult r = encode(&s->tmaps[st].m[f], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, src[st][f], dims, strides,
-                                box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS) return;
-    }
+    for (int f = 0; f < 4; f++)
+      if (!encode_field(encode, s, &s->tmaps[st].m[f], src[st][f], swe::SSXT, swe::SSY)) return;
   s->tma = 1;
 }
 
@@ -366,6 +405,7 @@ int ensure_split(swe_sim* s) {
   s->sb.nty = (int)s->sgrid.y;
   s->d_odry[0] = reinterpret_cast<int*>(s->d_split + swe::SPLIT_FIELDS * N + (ntiles + 1) / 2);
   s->d_odry[1] = reinterpret_cast<int*>(s->d_split + swe::SPLIT_FIELDS * N + 2 * ((ntiles + 1) / 2));
+  make_cell_maps(s);
   return SWE_OK;
 }
 
@@ -380,9 +420,17 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
     const dim3 blk(swe::SP_THREADS);
     if (s->tma) CU(launch(pdl, swe::k_split_faces_tma, s->sgrid, blk, s->st, a, sb, s->d_ctl, s->tmaps[MODE - 1]));
     else CU(launch(pdl, swe::k_split_faces, s->sgrid, blk, s->st, a, sb, s->d_ctl));
-    if (s->settle) CU(launch(pdl, swe::k_split_cells<MODE, true>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
-    else CU(launch(pdl, swe::k_split_cells<MODE, false>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
-    CU(launch(pdl, swe::k_split_close<MODE>, dim3(1), blk, s->st, a, s->d_ctl, (int)(s->sgrid.x * s->sgrid.y)));
+    if (s->cell_tma) {
+      const swe::CellMaps& cm = s->cmaps[MODE - 1];
+      if (s->settle) CU(launch(pdl, swe::k_split_cells_tma<MODE, true>, s->sgrid, blk, s->st, a, sb, s->d_ctl, cm));
+      else CU(launch(pdl, swe::k_split_cells_tma<MODE, false>, s->sgrid, blk, s->st, a, sb, s->d_ctl, cm));
+    } else if (s->settle) {
+      CU(launch(pdl, swe::k_split_cells<MODE, true>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
+    } else {
+      CU(launch(pdl, swe::k_split_cells<MODE, false>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
+    }
+    CU(launch(pdl, swe::k_split_close_multi<MODE>, dim3(swe::CLOSE_BLOCKS), blk, s->st, a, s->d_ctl,
+              (int)(s->sgrid.x * s->sgrid.y), s->d_part + 3 * (size_t)s->part_cap));
   } else {
     swe::k_stage<MODE><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a, s->d_ctl);
   }
@@ -578,11 +626,11 @@ int swe_create(const swe_options* o, const double* b, const double* h, swe_sim**
   CUB(cudaMalloc(&s->d_b, nb));
   for (int q = 0; q < 3; q++) { CUB(cudaMalloc(&s->d_A[q], nb)); CUB(cudaMalloc(&s->d_B[q], nb)); }
   CUB(cudaMalloc(&s->d_geom, sizeof(double) * (SWE_GEOM_NROWS + 3) * s->H));
-  CUB(cudaMalloc(&s->d_part, sizeof(double) * 3 * s->part_cap));
+  CUB(cudaMalloc(&s->d_part, sizeof(double) * (3 * s->part_cap + 2 * swe::CLOSE_BLOCKS)));   // + the close's scratch
   CUB(cudaMalloc(&s->d_rows, sizeof(double) * std::max(1, s->ny)));
   CUB(cudaMalloc(&s->d_ctl, sizeof(swe::Control)));
   CUB(cudaMemsetAsync(s->d_ctl, 0, sizeof(swe::Control), s->st));
-  CUB(cudaMemsetAsync(s->d_part, 0, sizeof(double) * 3 * s->part_cap, s->st));
+  CUB(cudaMemsetAsync(s->d_part, 0, sizeof(double) * (3 * s->part_cap + 2 * swe::CLOSE_BLOCKS), s->st));
   for (int q = 0; q < 3; q++) {
     CUB(cudaMemsetAsync(s->d_A[q], 0, nb, s->st));
     CUB(cudaMemsetAsync(s->d_B[q], 0, nb, s->st));

@@ -600,7 +600,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, Control* ctl, int
               const double u = qdiv(vel_num(nhu, nh), den), v = qdiv(vel_num(nhv, nh), den);
               const double speed = hypot(u, v);
               if (!(speed < 1e-14)) {
-                const double denom = 1 + dt * SWE_G * n * n * speed / pow(nh, 4.0 / 3.0);
+                const double denom = 1 + dt * SWE_G * n * n * speed / pow43(nh);
                 nhu = qdiv(nhu, denom);
                 nhv = qdiv(nhv, denom);
               }
@@ -820,7 +820,7 @@ __global__ void k_friction(StageArgs a, double dt) {
     const double u = vel_num(a.ohu[k], hk) / den, v = vel_num(a.ohv[k], hk) / den;
     const double speed = hypot(u, v);
     if (speed < 1e-14) continue;
-    const double denom = 1 + dt * SWE_G * n * n * speed / pow(hk, 4.0 / 3.0);
+    const double denom = 1 + dt * SWE_G * n * n * speed / pow43(hk);
     a.ohu[k] = a.ohu[k] / denom;
     a.ohv[k] = a.ohv[k] / denom;
   }

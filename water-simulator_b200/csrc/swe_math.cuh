@@ -54,6 +54,13 @@ __device__ __forceinline__ double qdiv(double x, double y) {
   return z ? __longlong_as_double(xb ^ (yb & 0x8000000000000000ull)) : q;
 }
 
+// h^(4/3) of Manning friction (src/swe.mjs:683, 699: Math.pow(hk, 4 / 3)) as
+// h * cbrt(h): within about 2 ulp of the power, as CUDA's pow is (the
+// reference's Math.pow is not correctly rounded either, so friction is held
+// to a tolerance rather than to the bits), at a fraction of pow's cost.
+// Callers pass h > minDepth >= 0.
+__device__ __forceinline__ double pow43(double h) { return h * cbrt(h); }
+
 // Limiters, src/swe.mjs:88-141.  lim: 0 mc (default), 1 minmod, 2 central.
 __device__ __forceinline__ double limiter(int lim, double a, double b) {
   if (lim == 0) {                                   // mc, src/swe.mjs:133-138

@@ -441,6 +441,24 @@ struct CellsSmem {
   bool last;
 };
 
+// The cell kernel's inputs from the face kernel, staged by tensor-map copies
+// for the tile at (i0, j0) (TMA variant): the mass fluxes of every face the
+// limiter ring and the gather touch, the other face values of the gather and
+// the depths of the ring.  x = i0 - 2 (even) for every box but yt's; cells
+// outside the grid read as zeros, which the dry flags replace in any case.
+struct CellFaceTiles {
+  alignas(128) double xm[SPY + 2][SPX + 4];      // fx M, rows j0-1.., columns i0-2..
+  alignas(128) double ym[SPY + 3][SPX + 4];      // fy M, rows j0-2.., columns i0-2..
+  alignas(128) double hr[SPY + 2][SPX + 4];      // h of the stage input, rows j0-1.., columns i0-2..
+  alignas(128) double xt[3][SPY][SPX + 2];       // fx T, N + pL, N + pR, rows j0.., columns i0-2..
+  alignas(128) double yt[3][SPY + 1][SPX];       // fy T, N + pL, N + pR, rows j0-1.., columns i0..
+};
+enum { CM_XM, CM_YM, CM_H, CM_XT, CM_YT = CM_XT + 3, CM_COUNT = CM_YT + 3 };
+struct CellMaps { CUtensorMap m[CM_COUNT]; };
+constexpr unsigned CELL_TX_BYTES = sizeof(double) * (unsigned)((SPY + 2) * (SPX + 4) + (SPY + 3) * (SPX + 4) +
+                                                               (SPY + 2) * (SPX + 4) + 3 * SPY * (SPX + 2) +
+                                                               3 * (SPY + 1) * SPX);
+
 // A face / source-term value owned by cell (gi, gj) of the 3 x 3 tile
 // neighbourhood of the tile at (i0, j0): +0 when its tile was dry.
 __device__ __forceinline__ double split_load(const CellsSmem& sm, int i0, int j0, int gi, int gj,
@@ -462,6 +480,37 @@ __device__ __forceinline__ double split_theta(const StageArgs& a, const SplitBuf
   const double fyN = split_load(sm, i0, j0, gi, gj, s.fy[F_M], k);
   const double fyS = split_load(sm, i0, j0, gi, gj - 1, s.fy[F_M], k - W);
   const double avail = a.h[k];
+  const double est = ((fxE > 0 ? fxE : 0) - (fxW < 0 ? fxW : 0)) * a.m.rdxRow[gj]
+                   + (fyN > 0 ? fyN : 0) * a.m.rdyRowN[gj] - (fyS < 0 ? fyS : 0) * a.m.rdyRowS[gj];
+  double th = 1;
+  if (!(est * dt * (1 + 1e-12) < avail)) {
+    double out = 0;
+    if (fxE > 0) out += fxE / a.m.dxRow[gj];
+    if (fxW < 0) out -= fxW / a.m.dxRow[gj];
+    if (fyN > 0) out += fyN / a.m.dyRowN[gj];
+    if (fyS < 0) out -= fyS / a.m.dyRowS[gj];
+    if (out * dt > avail) th = avail > 0 ? avail / (out * dt) : 0;
+  }
+  return th;
+}
+
+// split_theta from the staged tiles: the same values, read from shared
+// memory (+0 where split_load gives +0).
+__device__ __forceinline__ bool split_dry_at(const CellsSmem& sm, int i0, int j0, int gi, int gj) {
+  const int c = gi < i0 ? 0 : (gi >= i0 + SPX ? 2 : 1);
+  const int r = gj < j0 ? 0 : (gj >= j0 + SPY ? 2 : 1);
+  return sm.dry[r][c] != 0;
+}
+__device__ __forceinline__ double split_theta_st(const StageArgs& a, const CellFaceTiles& ft, const CellsSmem& sm,
+                                                 int i0, int j0, double dt, int gi, int gj) {
+  const int W = a.W, H = a.H;
+  if (!(dt > 0 && gj >= 1 && gj < H - 1 && gi >= 1 && gi < W - 1)) return 1;
+  const int cx = gi - i0 + 2, rx = gj - j0 + 1, ry = gj - j0 + 2;
+  const double fxE = split_dry_at(sm, i0, j0, gi, gj) ? 0.0 : ft.xm[rx][cx];
+  const double fxW = split_dry_at(sm, i0, j0, gi - 1, gj) ? 0.0 : ft.xm[rx][cx - 1];
+  const double fyN = split_dry_at(sm, i0, j0, gi, gj) ? 0.0 : ft.ym[ry][cx];
+  const double fyS = split_dry_at(sm, i0, j0, gi, gj - 1) ? 0.0 : ft.ym[ry - 1][cx];
+  const double avail = ft.hr[rx][cx];
   const double est = ((fxE > 0 ? fxE : 0) - (fxW < 0 ? fxW : 0)) * a.m.rdxRow[gj]
                    + (fyN > 0 ? fyN : 0) * a.m.rdyRowN[gj] - (fyS < 0 ? fyS : 0) * a.m.rdyRowS[gj];
   double th = 1;
@@ -536,10 +585,11 @@ __device__ __forceinline__ void split_close_block(const StageArgs& a, Control* c
 // metrics (StageArgs::dryfold) each face term is then +0 * (finite) = +-0
 // added to or taken from a +0 sum, and the bed terms are +0, so the sums
 // are +0 with or without them: DRY leaves them out and gives the same bits.
-template <int MODE, bool DRY>
+// ST: the face values come from the staged tiles ft.
+template <int MODE, bool DRY, bool ST = false>
 __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& s, const CellsSmem& sm, int t,
                                            int lx, int ly, int gi, int gj, double dt, double& locMax,
-                                           double& locFl, double& hout) {
+                                           double& locFl, double& hout, const CellFaceTiles* ft = nullptr) {
   const int W = a.W, H = a.H;
   const double dry = a.minDepth, eps4 = a.eps4;
   const bool sph = a.sph != 0;
@@ -553,10 +603,17 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
   const bool interior = colY && rowX;
   double wM = 0, wT = 0, wN = 0, eM = 0, eT = 0, eN = 0, sM = 0, sT = 0, sN = 0, nM = 0, nT = 0, nN = 0;
   const bool dW = sm.dry[1][lx == 0 ? 0 : 1], dS = sm.dry[ly == 0 ? 0 : 1][1], dC = sm.dry[1][1];
-  if (!DRY && hasW && !dW) { wM = s.fx[F_M][k - 1]; wT = s.fx[F_T][k - 1]; wN = s.fx[F_NPR][k - 1]; }
-  if (!DRY && hasE && !dC) { eM = s.fx[F_M][k]; eT = s.fx[F_T][k]; eN = s.fx[F_NPL][k]; }
-  if (!DRY && hasS && !dS) { sM = s.fy[F_M][k - W]; sT = s.fy[F_T][k - W]; sN = s.fy[F_NPR][k - W]; }
-  if (!DRY && hasN && !dC) { nM = s.fy[F_M][k]; nT = s.fy[F_T][k]; nN = s.fy[F_NPL][k]; }
+  if (ST) {
+    if (!DRY && hasW && !dW) { wM = ft->xm[ly + 1][lx + 1]; wT = ft->xt[0][ly][lx + 1]; wN = ft->xt[2][ly][lx + 1]; }
+    if (!DRY && hasE && !dC) { eM = ft->xm[ly + 1][lx + 2]; eT = ft->xt[0][ly][lx + 2]; eN = ft->xt[1][ly][lx + 2]; }
+    if (!DRY && hasS && !dS) { sM = ft->ym[ly + 1][lx + 2]; sT = ft->yt[0][ly][lx]; sN = ft->yt[2][ly][lx]; }
+    if (!DRY && hasN && !dC) { nM = ft->ym[ly + 2][lx + 2]; nT = ft->yt[0][ly + 1][lx]; nN = ft->yt[1][ly + 1][lx]; }
+  } else {
+    if (!DRY && hasW && !dW) { wM = s.fx[F_M][k - 1]; wT = s.fx[F_T][k - 1]; wN = s.fx[F_NPR][k - 1]; }
+    if (!DRY && hasE && !dC) { eM = s.fx[F_M][k]; eT = s.fx[F_T][k]; eN = s.fx[F_NPL][k]; }
+    if (!DRY && hasS && !dS) { sM = s.fy[F_M][k - W]; sT = s.fy[F_T][k - W]; sN = s.fy[F_NPR][k - W]; }
+    if (!DRY && hasN && !dC) { nM = s.fy[F_M][k]; nT = s.fy[F_T][k]; nN = s.fy[F_NPL][k]; }
+  }
   cp_async_wait_all();
   const double hin = sm.st[0][t], huin = sm.st[1][t], hvin = sm.st[2][t];
   double tb0 = 0, tb1 = 0, tg = 0, Uk = 0;
@@ -636,7 +693,7 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
           const double u = qdiv(vel_num(nhu, nh), den), v = qdiv(vel_num(nhv, nh), den);
           const double speed = hypot(u, v);
           if (!(speed < 1e-14)) {
-            const double denom = 1 + dt * SWE_G * n * n * speed / pow(nh, 4.0 / 3.0);
+            const double denom = 1 + dt * SWE_G * n * n * speed / pow43(nh);
             nhu = qdiv(nhu, denom);
             nhv = qdiv(nhv, denom);
           }
@@ -676,9 +733,15 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
 // by k_split_close after the launch.  Every thread of the CTA calls it.
 // SETTLE: tiles may settle (below); without it the function is the plain
 // tile update, which grids with little dry land run faster.
-template <int MODE, bool SETTLE = false>
+// TMA: the limiter ring's and the gather's inputs are staged into ft by
+// tensor-map copies (maps, completing on bar) once the tile is known to be
+// computed; a copy that does not complete within the bound sets bit 4 of
+// Control::status and leaves the tile's output unwritten.
+template <int MODE, bool SETTLE = false, bool TMA = false>
 __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const SplitBufs& s, Control* ctl, int tx,
-                                                 int ty, int part, int nparts, CellsSmem& sm, bool ticket) {
+                                                 int ty, int part, int nparts, CellsSmem& sm, bool ticket,
+                                                 CellFaceTiles* ft = nullptr, const CellMaps* maps = nullptr,
+                                                 unsigned long long* bar = nullptr) {
   static_assert(MODE == 1 || MODE == 2, "stages only");
   const int W = a.W, H = a.H;
   const int i0 = tx * SPX, j0 = ty * SPY;
@@ -763,10 +826,34 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
       cp_async8(&sm.st[5][t], a.ohv + k);
     }
   }
+  if (TMA && !fold) {
+    if (t == 0) {
+      // the generic-proxy accesses of the shared memory come before the copies' writes
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      mbar_expect_tx(bar, CELL_TX_BYTES);
+      const int x = i0 - 2;
+      tma_load_tile(&ft->xm[0][0], &maps->m[CM_XM], x, j0 - 1, bar);
+      tma_load_tile(&ft->ym[0][0], &maps->m[CM_YM], x, j0 - 2, bar);
+      tma_load_tile(&ft->hr[0][0], &maps->m[CM_H], x, j0 - 1, bar);
+      for (int q = 0; q < 3; q++) {
+        tma_load_tile(&ft->xt[q][0][0], &maps->m[CM_XT + q], x, j0, bar);
+        tma_load_tile(&ft->yt[q][0][0], &maps->m[CM_YT + q], i0, j0 - 1, bar);
+      }
+    }
+    const bool ok = mbar_wait_bounded(bar, 0, TMA_WAIT_TRIES);
+    if (!__syncthreads_and(ok)) {                   // uniform: give up on the tile
+      if (t == 0) atomicOr(&ctl->status, 4);
+      mbar_wait_bounded(bar, 0, TMA_WAIT_TRIES);    // let a late copy land first
+      cp_async_wait_all();
+      __syncthreads();
+      return;
+    }
+  }
   if (!fold) {
     for (int q = t; q < (SPX + 2) * (SPY + 2); q += SP_THREADS) {
       const int ly = q / (SPX + 2), lx = q - ly * (SPX + 2);
-      sm.th[ly][lx] = allDry ? 1.0 : split_theta(a, s, sm, i0, j0, dt, i0 - 1 + lx, j0 - 1 + ly);
+      if (TMA) sm.th[ly][lx] = allDry ? 1.0 : split_theta_st(a, *ft, sm, i0, j0, dt, i0 - 1 + lx, j0 - 1 + ly);
+      else sm.th[ly][lx] = allDry ? 1.0 : split_theta(a, s, sm, i0, j0, dt, i0 - 1 + lx, j0 - 1 + ly);
     }
     __syncthreads();
   }
@@ -774,7 +861,7 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
   double locMax = 0, locFl = 0, hout = 0;
   if (gi < W && gj < H) {
     if (fold) split_cell<MODE, true>(a, s, sm, t, lx, ly, gi, gj, dt, locMax, locFl, hout);
-    else split_cell<MODE, false>(a, s, sm, t, lx, ly, gi, gj, dt, locMax, locFl, hout);
+    else split_cell<MODE, false, TMA>(a, s, sm, t, lx, ly, gi, gj, dt, locMax, locFl, hout, ft);
   }
   if (s.odry_out) {                               // the written tile's flag
     const bool ghostFree = i0 >= 2 && i0 + SPX <= W - 2 && j0 >= 2 && j0 + SPY <= H - 2;
@@ -826,6 +913,84 @@ k_split_cells(StageArgs a, SplitBufs s, Control* ctl) {
   __shared__ CellsSmem sm;
   split_cells_tile<MODE, SETTLE>(a, s, ctl, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
                          gridDim.x * gridDim.y, sm, false);
+}
+
+// The close of a stage over CLOSE_BLOCKS blocks: block b reduces its run of
+// the tiles' partial slots (strided per thread, then a fixed tree) into
+// scratch, and the last block to finish (a ticket among the CLOSE_BLOCKS)
+// combines the blocks' results in block order (a fixed tree in one warp)
+// and closes the stage as split_close_block does.  The maximum is the same
+// in any order; the floored mass is summed in this fixed order.  One block
+// reading 16 705 slots spent most of its time in dependent rounds of L2
+// loads.  scratch holds 2 * CLOSE_BLOCKS doubles.
+constexpr int CLOSE_BLOCKS = 32;
+template <int MODE>
+__global__ void __launch_bounds__(SP_THREADS) k_split_close_multi(StageArgs a, Control* ctl, int nparts,
+                                                                    double* scratch) {
+  pdl_enter();
+  if (ctl->stop) return;
+  __shared__ double red[2][SP_THREADS / 32];
+  __shared__ int last;
+  const int t = threadIdx.x, b = blockIdx.x;
+  const int chunk = (nparts + CLOSE_BLOCKS - 1) / CLOSE_BLOCKS;
+  const int q0 = b * chunk, q1 = min(nparts, q0 + chunk);
+  const double* pf = MODE == 1 ? a.part_fl1 : a.part_fl2;
+  double m = 0, f = 0;
+  for (int q = q0 + t; q < q1; q += SP_THREADS) {
+    if (MODE == 2) m = fmax(m, __ldcg(a.part_max + q));
+    f += __ldcg(pf + q);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    f += __shfl_down_sync(0xffffffffu, f, o);
+  }
+  if ((t & 31) == 0) { red[0][t >> 5] = m; red[1][t >> 5] = f; }
+  __syncthreads();
+  if (t == 0) {
+    m = red[0][0]; f = red[1][0];
+    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, red[0][w]); f += red[1][w]; }
+    scratch[b] = m;
+    scratch[CLOSE_BLOCKS + b] = f;
+    __threadfence();
+    last = atomicAdd(&ctl->counter, 1u) == (unsigned int)(CLOSE_BLOCKS - 1);
+  }
+  __syncthreads();
+  if (!last || t >= 32) return;                   // uniform per block; warp 0 of the last block goes on
+  __threadfence();
+  static_assert(CLOSE_BLOCKS == 32, "one block result per lane");
+  m = __ldcg(scratch + t);
+  f = __ldcg(scratch + CLOSE_BLOCKS + t);
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    f += __shfl_down_sync(0xffffffffu, f, o);
+  }
+  if (t == 0) {
+    const double dt = ctl->dt;
+    if (MODE == 1) {
+      ctl->floored1 = f;
+    } else {
+      ctl->next_max = m;
+      ctl->mass_floored = ctl->floored1 + f;
+      ctl->t = ctl->t + dt;
+      ctl->steps = ctl->steps + 1;
+    }
+    ctl->counter = 0;
+  }
+}
+
+// The cell kernel with its face and depth inputs staged by tensor-map copies
+// (maps over this simulation's own buffers only, no multicast).
+template <int MODE, bool SETTLE = false>
+__global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_CELLS_MIN_BLOCKS)
+k_split_cells_tma(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant__ CellMaps maps) {
+  __shared__ CellsSmem sm;
+  __shared__ CellFaceTiles ft;
+  __shared__ alignas(8) unsigned long long bar;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);        // before the wait: touches no global memory
+  pdl_enter();
+  if (ctl->stop) return;
+  split_cells_tile<MODE, SETTLE, true>(a, s, ctl, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
+                                       gridDim.x * gridDim.y, sm, false, &ft, &maps, &bar);
 }
 
 // Closes the stage k_split_cells left open: one block, no atomics (a
