@@ -540,6 +540,7 @@ def run_ours(args):
         extras["all_wet"] = all_wet_summary(torch, swe, max(K, 200), local)
         extras["batched"] = ensemble_summary(torch, swe, device=local)
         extras["adjoint"] = adjoint_summary(torch, swe, device=local)
+        extras["fma_build"] = fma_build_summary(K, args.warmup)
 
     if world > 1:
         torch.distributed.barrier()
@@ -565,6 +566,30 @@ def run_ours(args):
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def fma_build_summary(steps, warmup):
+    """The production build (libswe_b200_fma.so, -fmad=true: the compiler
+    fuses multiply-adds; held to 1e-12 per step against the oracle by its
+    own test) on the same beach steps and on the all-wet grid, each in a
+    child process, since a process loads one build."""
+    lib = os.path.join(ROOT, "water-simulator_b200", "libswe_b200_fma.so")
+    if not os.path.exists(lib):
+        return {"unavailable": "libswe_b200_fma.so is not built"}
+    env = dict(os.environ, SWE_B200_ARITH="fma")
+    out = {"how": "bench.py in a child process with SWE_B200_ARITH=fma"}
+    for key, extra in (("value", ["--no-cpu-baseline", "--no-extras", "--steps", str(steps), "--warmup", str(warmup)]),
+                       ("all_wet", ["--workload", "allwet", "--steps", "200", "--warmup", "32"])):
+        try:
+            r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py")] + extra, env=env,
+                               capture_output=True, text=True, timeout=600)
+            lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+            out[key] = json.loads(lines[-1])["value"] if r.returncode == 0 and lines else None
+        except (subprocess.TimeoutExpired, ValueError, KeyError) as e:
+            out[key] = None
+            out[key + "_error"] = str(e)[:200]
+    out["unit"] = UNIT
+    return out
 
 
 def launches_per_step(swe, lib, sim):
@@ -604,7 +629,7 @@ def run_ensemble(args):
     mine = sharding.assign_basins([b["nx"] * b["ny"] for b in all_bs], world)[rank]
     bs = [all_bs[q] for q in mine]
     cells = sum(b["nx"] * b["ny"] for b in bs)
-    K = max(4, min(args.steps, 64))
+    K = max(4, min(args.steps, 1000))               # the configuration's 1000 steps by default
     ens = swe.Ensemble(bs)
     tuned = ens.autotune(trial_steps=3)
     ens.run(max(args.warmup, 3))
