@@ -324,8 +324,13 @@ int swe_adjoint_get_stream(swe_adjoint* s, void** stream);
  * boundary asks for a new forward pass before the next backward. */
 int swe_adjoint_set_boundary(swe_adjoint* s, int side, int kind);
 /* Flather on `side` with the constant exterior surface eta_ext and normal
- * velocity u_ext (src/swe.mjs:1085-1115; a tide signal is not covered). */
+ * velocity u_ext (src/swe.mjs:1085-1115). */
 int swe_adjoint_set_flather_values(swe_adjoint* s, int side, double eta_ext, double u_ext);
+/* Flather on `side` with the exterior state of a tide, as
+ * swe_set_flather_tide (src/tide.mjs:103-107): each step's values at its t
+ * are recorded by the forward and used by the reverse. */
+int swe_adjoint_set_flather_tide(swe_adjoint* s, int side, double msl, int n, const double* amp, const double* omega,
+                                 const double* phase_deg, double u_coef);
 
 /* ---- stage kernels -----------------------------------------------------------
  * Two implementations of each SSP-RK2 stage, bit-identical in their results:

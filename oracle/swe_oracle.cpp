@@ -940,22 +940,19 @@ void   oracle_hllc(double* out3, double hL, double huL, double hvL, double hR, d
 // oracle_tlm_misfit_bc: the same with a boundary kind per side (W, E, S, N:
 // OB_REFLECT, OB_OUTFLOW, OB_PERIODIC, OB_FLATHER) and, for Flather sides,
 // the constant exterior surface and normal velocity.
-int oracle_tlm_misfit_bc(const oracle_options* o, const double* b, const double* eta0, const double* n,
-                         const double* db, const double* dn, int ng, const int* gauges, int steps,
-                         const double* obs, int threads, const int* kinds, const double* fl_eta,
-                         const double* fl_u, double* J, double* dJ, double* dts);
 
 int oracle_tlm_misfit(const oracle_options* o, const double* b, const double* eta0, const double* n,
                       const double* db, const double* dn, int ng, const int* gauges, int steps,
                       const double* obs, int threads, double* J, double* dJ, double* dts) {
   return oracle_tlm_misfit_bc(o, b, eta0, n, db, dn, ng, gauges, steps, obs, threads, nullptr, nullptr, nullptr,
-                              J, dJ, dts);
+                              nullptr, J, dJ, dts);
 }
 
 int oracle_tlm_misfit_bc(const oracle_options* o, const double* b, const double* eta0, const double* n,
                          const double* db, const double* dn, int ng, const int* gauges, int steps,
                          const double* obs, int threads, const int* kinds, const double* fl_eta,
-                         const double* fl_u, double* J, double* dJ, double* dts) {
+                         const double* fl_u, const oracle_tide_spec* tides, double* J, double* dJ,
+                         double* dts) {
   if (!o || o->sphere || !b || !eta0 || !db || ng < 1 || !gauges || steps < 1 || !obs) {
     g_err = "oracle_tlm_misfit: Cartesian options, b, eta0, db, gauges, steps, obs"; return -1;
   }
@@ -967,6 +964,14 @@ int oracle_tlm_misfit_bc(const oracle_options* o, const double* b, const double*
     s.flTide[q] = false;
     s.flEta[q] = fl_eta ? fl_eta[q] : 0.0;
     s.flU[q] = fl_u ? fl_u[q] : 0.0;
+    if (tides && tides[q].n > 0 && kind == OB_FLATHER) {
+      const oracle_tide_spec& ts = tides[q];
+      s.flTide[q] = true;
+      s.tide[q].msl = ts.msl; s.tide[q].u_coef = ts.u_coef;
+      s.tide[q].amp.assign(ts.amp, ts.amp + ts.n);
+      s.tide[q].omega.assign(ts.omega, ts.omega + ts.n);
+      s.tide[q].phase.assign(ts.phase_deg, ts.phase_deg + ts.n);
+    }
   }
   s.nx = o->nx; s.ny = o->ny; s.ng = 2; s.W = s.nx + 4; s.H = s.ny + 4; s.N = s.W * s.H;
   s.dx = o->dx; s.dy = o->dy; s.manning = o->manning; s.minDepth = o->min_depth; s.cfl = o->cfl;

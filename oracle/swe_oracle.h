@@ -86,12 +86,20 @@ void         oracle_hllc(double* out3, double hL, double huL, double hvL, double
 int          oracle_tlm_misfit(const oracle_options* o, const double* b, const double* eta0, const double* n,
                                const double* db, const double* dn, int ng, const int* gauges, int steps,
                                const double* obs, int threads, double* J, double* dJ, double* dts);
-/* The same with a boundary kind per side (W, E, S, N; NULL: reflect) and the
- * constant Flather exterior surface and normal velocity (NULL: 0). */
+/* A Flather side's tide (src/tide.mjs:103-107): eta(t) = msl + sum amp cos(omega t - phase), u = u_coef eta. */
+typedef struct {
+  int n;                        /* constituents; 0: the side keeps its constant exterior state */
+  double msl, u_coef;
+  const double* amp; const double* omega; const double* phase_deg;
+} oracle_tide_spec;
+/* The same with a boundary kind per side (W, E, S, N; NULL: reflect), the
+ * constant Flather exterior surface and normal velocity (NULL: 0), and a
+ * tide per side (NULL, or n = 0: none). */
 int          oracle_tlm_misfit_bc(const oracle_options* o, const double* b, const double* eta0, const double* n,
                                   const double* db, const double* dn, int ng, const int* gauges, int steps,
                                   const double* obs, int threads, const int* kinds, const double* fl_eta,
-                                  const double* fl_u, double* J, double* dJ, double* dts);
+                                  const double* fl_u, const oracle_tide_spec* tides, double* J, double* dJ,
+                                  double* dts);
 
 #ifdef __cplusplus
 }

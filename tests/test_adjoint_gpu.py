@@ -112,13 +112,16 @@ BOUNDARY_CASES = {
     "flather_sn_periodic_we": {"south": ("flather", 2.0, 0.01), "north": ("flather", 1.95, -0.02),
                                "west": "periodic", "east": "periodic"},
     "mixed": {"east": ("flather", 2.0, 0.0), "south": "outflow", "north": "periodic"},
+    "tide_west": {"west": ("tide", 2.0, [0.3, 0.1], [2 * 3.141592653589793 / 600, 2 * 3.141592653589793 / 250],
+                           [0.0, 40.0], 0.05), "east": "outflow"},
 }
 
 
 @pytest.mark.parametrize("name", list(BOUNDARY_CASES))
 def test_adjoint_boundaries_match_tangent_linear(swe, name):
-    """Outflow, periodic and Flather sides (src/swe.mjs:1026-1126): the
-    forward equals the oracle's, the gradient its tangent-linear model."""
+    """Outflow, periodic and Flather sides, constant or tidal
+    (src/swe.mjs:1026-1126): the forward equals the oracle's, the gradient
+    its tangent-linear model."""
     from water_simulator_b200 import workloads
     bcs = BOUNDARY_CASES[name]
     steps, nx, ny = 24, 40, 30

@@ -34,13 +34,15 @@ def test_tlm_matches_central_differences():
 
 
 def test_tlm_with_open_boundaries_matches_central_differences():
-    """The same with outflow, periodic and constant-state Flather sides."""
+    """The same with outflow, periodic and Flather sides (constant and tidal)."""
     case = small_case()
     steps = 20
     rng = np.random.default_rng(4)
     obs = rng.normal(2.0, 0.05, (steps, len(case["gauges"])))
+    tide = ("tide", 2.0, [0.3, 0.1], [2 * np.pi / 600, 2 * np.pi / 250], [0.0, 40.0], 0.05)
     for bcs in ({"west": ("flather", 2.05, 0.0), "east": "outflow", "south": "periodic", "north": "periodic"},
-                {"south": ("flather", 1.95, -0.02), "north": "outflow", "west": "periodic", "east": "periodic"}):
+                {"south": ("flather", 1.95, -0.02), "north": "outflow", "west": "periodic", "east": "periodic"},
+                {"west": tide, "east": "outflow"}):
         db = rng.normal(0, 1, case["b"].shape)
         dn = rng.normal(0, 1e-3, case["n"].shape)
         J, dJ, dts = tlm_misfit(case, case["b"], case["n"], db, dn, steps, obs, bcs=bcs)

@@ -147,6 +147,7 @@ SIGNATURES = {
     "swe_adjoint_get_stream": [_P, ctypes.POINTER(_P)],
     "swe_adjoint_set_boundary": [_P, _I, _I],
     "swe_adjoint_set_flather_values": [_P, _I, _D, _D],
+    "swe_adjoint_set_flather_tide": [_P, _I, _D, _I, _DP, _DP, _DP, _D],
 }
 _RESTYPES = {"swe_last_error": ctypes.c_char_p}
 

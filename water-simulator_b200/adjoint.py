@@ -47,18 +47,26 @@ class MisfitAdjoint:
 
     def set_boundary(self, side, bc):
         """side: "west", "east", "south" or "north"; bc: "reflect", "outflow",
-        "periodic", or ("flather", eta_ext, u_ext) with a constant exterior
-        state (src/swe.mjs:1026-1126)."""
+        "periodic", ("flather", eta_ext, u_ext) with a constant exterior
+        state, or ("tide", msl, amps, omegas, phases_deg, u_coef): Flather
+        with the exterior state of a tide (src/swe.mjs:1026-1126,
+        src/tide.mjs:103-107)."""
         s = SIDES[side]
+        usage = "reflect, outflow, periodic, ('flather', eta, u) or ('tide', msl, amps, omegas, phases, u_coef)"
         if isinstance(bc, str):
             if bc not in ("reflect", "outflow", "periodic"):
-                raise ValueError(f"boundary {bc!r}: reflect, outflow, periodic or ('flather', eta, u)")
+                raise ValueError(f"boundary {bc!r}: {usage}")
             check(self._lib.swe_adjoint_set_boundary(self._h, s, BC_KIND[bc]))
+        elif bc[0] == "flather" and len(bc) == 3:
+            check(self._lib.swe_adjoint_set_flather_values(self._h, s, float(bc[1]), float(bc[2])))
+        elif bc[0] == "tide" and len(bc) == 6:
+            amp, om, ph = (np.ascontiguousarray(x, dtype=np.float64).reshape(-1) for x in bc[2:5])
+            if not (len(amp) == len(om) == len(ph)):
+                raise ValueError("tide: amps, omegas and phases differ in length")
+            check(self._lib.swe_adjoint_set_flather_tide(self._h, s, float(bc[1]), len(amp), dptr(amp), dptr(om),
+                                                         dptr(ph), float(bc[5])))
         else:
-            kind, eta_ext, u_ext = bc
-            if kind != "flather":
-                raise ValueError(f"boundary {bc!r}: reflect, outflow, periodic or ('flather', eta, u)")
-            check(self._lib.swe_adjoint_set_flather_values(self._h, s, float(eta_ext), float(u_ext)))
+            raise ValueError(f"boundary {bc!r}: {usage}")
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

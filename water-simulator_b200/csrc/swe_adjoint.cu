@@ -17,8 +17,8 @@
 // part of the map from b to J.
 //
 // Scope: Cartesian grids; per side reflect (the default), outflow, periodic
-// or Flather with a constant exterior state; any order and limiter,
-// Coriolis, scalar or per-cell Manning n.  No sponge or Flather tide.
+// or Flather with a constant exterior state or a tide; any order and
+// limiter, Coriolis, scalar or per-cell Manning n.  No sponge.
 #include "../../include/swe_b200.h"
 #include "swe_kernels.cuh"
 #include "swe_split.cuh"
@@ -45,8 +45,12 @@ using swe::pdl_enter;
 
 int fail(int code, const std::string& m) { swe_host::set_error(m); return code; }
 
-// The constant exterior state of the Flather sides (eta, normal velocity).
-struct FlatherValues { double eta[4], u[4]; };
+// Per step, what the step's prepare left in the control block: t at the
+// start of the step, then the Flather sides' exterior eta[4] and u[4]
+// (constants, or a tide at t).  The forward records it; the tape pass
+// starts each segment from its t, and the reverse of the ghost fill reads
+// the exterior state of the step it reverses.
+constexpr int STEP_REC = 9;
 
 #define CU(call)                                                                      \
   do {                                                                                \
@@ -496,7 +500,7 @@ __device__ __forceinline__ void flather_rev(int side, double e0, double u0, doub
 // map: sources[nsrc], offsets[nsrc + 1], ghosts[n], transforms[n] (padded
 // cell indices; swe::GT_*).  X: the stage input the fill was applied to.
 __global__ void k_adj_bc(int nsrc, const int* map, const double* b, const double* h, const double* hu,
-                         const double* hv, FlatherValues fv, double minDepth, double eps4, double* lb, double* lh,
+                         const double* hv, const double* fl, double minDepth, double eps4, double* lb, double* lh,
                          double* lhu, double* lhv) {
   pdl_enter();
   const int* src = map;
@@ -512,7 +516,7 @@ __global__ void k_adj_bc(int nsrc, const int* map, const double* b, const double
       lb[gk] = 0; lh[gk] = 0; lhu[gk] = 0; lhv[gk] = 0;
       if (tr >= swe::GT_FLATHER) {
         const int side = tr - swe::GT_FLATHER;
-        flather_rev(side, fv.eta[side], fv.u[side], minDepth, eps4, b[sk], h[sk], hu[sk], hv[sk], Lb, Lh, Lhu,
+        flather_rev(side, fl[side], fl[4 + side], minDepth, eps4, b[sk], h[sk], hu[sk], hv[sk], Lb, Lh, Lhu,
                     Lhv, ab, ah, ahu, ahv);
       } else {
         ab += Lb;
@@ -642,12 +646,18 @@ __global__ void k_adj_misfit(const double* b, const double* h, const int* gcell,
     lb[k] = ab;
   }
 }
-__global__ void k_set_dt(Control* ctl, const double* dts, int s, FlatherValues fv) {
+// After a step's prepare: t and the Flather exterior state into rec (STEP_REC doubles).
+__global__ void k_record_step(const Control* ctl, double* rec) {
   pdl_enter();
   if (threadIdx.x == 0) {
-    ctl->dt = dts[s]; ctl->stop = 0;
-    for (int q = 0; q < 4; q++) { ctl->fl_eta[q] = fv.eta[q]; ctl->fl_u[q] = fv.u[q]; }
+    rec[0] = ctl->t;
+    for (int q = 0; q < 4; q++) { rec[1 + q] = ctl->fl_eta[q]; rec[5 + q] = ctl->fl_u[q]; }
   }
+}
+// The time of the step a segment's tape pass starts with.
+__global__ void k_set_t(Control* ctl, const double* rec) {
+  pdl_enter();
+  if (threadIdx.x == 0) ctl->t = rec[0];
 }
 __global__ void k_record_dt(const Control* ctl, double* dts, int s) {
   pdl_enter();
@@ -706,7 +716,10 @@ struct swe_adjoint {
   bool pdl = true;                 // programmatic dependent launch between the stepping kernels
   bool fixed_dt = false;         // forward uses the given dt sequence instead of maxDt()
   int kind[4] = {SWE_BC_REFLECT, SWE_BC_REFLECT, SWE_BC_REFLECT, SWE_BC_REFLECT};   // W, E, S, N
-  FlatherValues flv = {};        // exterior state of the Flather sides
+  double fl_eta[4] = {0, 0, 0, 0}, fl_u[4] = {0, 0, 0, 0};   // constant exterior state of the Flather sides
+  int fl_kind[4] = {0, 0, 0, 0};  // 1: the side's exterior state is the tide of ctl_init
+  Control ctl_init = {};          // the control block each forward starts from (tide tables, zeros)
+  double* rec = nullptr;          // STEP_REC doubles per step
   int* gmap = nullptr;           // the ghost fill by source (k_adj_bc)
   int nsrc = 0;
   std::vector<double> dts_host;  // the dt sequence, read once per backward pass
@@ -784,18 +797,24 @@ int copy3(swe_adjoint* s, double* const* dst, double* const* src, bool pdl = tru
   return SWE_OK;
 }
 
-// One forward step of state X in place, dt from the device control block
-// (set by k_set_dt or, when auto_dt, from the CFL rate).
+// The step's prepare: dt = maxDt() from the CFL rate (auto_dt) or the
+// recorded dt of step k, and the Flather exterior state at the control
+// block's t.
+swe::PrepArgs prep_of(const swe_adjoint* s, bool auto_dt, int k) {
+  swe::PrepArgs p;
+  std::memset(&p, 0, sizeof p);
+  p.mode = auto_dt ? 1 : 4;
+  p.cfl = s->o.cfl;
+  p.t_end = INFINITY;
+  p.dt_dev = s->dts + k;
+  for (int q = 0; q < 4; q++) { p.fl_kind[q] = s->fl_kind[q]; p.fl_eta[q] = s->fl_eta[q]; p.fl_u[q] = s->fl_u[q]; }
+  return p;
+}
+
+// One forward step of state X in place.
 int fwd_step(swe_adjoint* s, double* const* X, bool auto_dt, int step_index) {
-  if (auto_dt) {
-    swe::PrepArgs p;
-    std::memset(&p, 0, sizeof p);
-    p.mode = 1; p.cfl = s->o.cfl; p.t_end = INFINITY;
-    for (int q = 0; q < 4; q++) { p.fl_eta[q] = s->flv.eta[q]; p.fl_u[q] = s->flv.u[q]; }
-    LAUNCH(swe::k_prepare, dim3(1), dim3(32), s->ctl, p);
-  } else {
-    LAUNCH(k_set_dt, dim3(1), dim3(32), s->ctl, (const double*)s->dts, step_index, s->flv);
-  }
+  LAUNCH(swe::k_prepare, dim3(1), dim3(32), s->ctl, prep_of(s, auto_dt, step_index));
+  LAUNCH(k_record_step, dim3(1), dim3(32), (const Control*)s->ctl, s->rec + (size_t)STEP_REC * step_index);
   const dim3 spb(swe::SP_THREADS);
   const int nparts = (int)(s->sgrid.x * s->sgrid.y);
   LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, X), (const Control*)s->ctl, 0);
@@ -887,7 +906,8 @@ swe::SplitBufs tape_bufs(const swe_adjoint* s, const Inter& it) {
 int tape_step(swe_adjoint* s, double* const* X, int k, const Tape& T) {
   const dim3 spb(swe::SP_THREADS);
   const int nparts = (int)(s->sgrid.x * s->sgrid.y);
-  LAUNCH(k_set_dt, dim3(1), dim3(32), s->ctl, (const double*)s->dts, k, s->flv);
+  if (k % s->every == 0) LAUNCH(k_set_t, dim3(1), dim3(32), s->ctl, (const double*)(s->rec + (size_t)STEP_REC * k));
+  LAUNCH(swe::k_prepare, dim3(1), dim3(32), s->ctl, prep_of(s, false, k));
   // the step input with its ghosts, in X (U0 of the in-place stage 2) and on the tape
   LAUNCH(swe::k_apply_bc, dim3(bcb(s)), dim3(256), bc_args(s, X), (const Control*)s->ctl, 0);
   if (int rc = copy3(s, T.W1, X)) return rc;
@@ -926,7 +946,8 @@ int reverse_step(swe_adjoint* s, int k, const Tape& T) {
   int rc = residual_adjoint(s, T.Bp, T.it2, T.th2, dt, lB);
   if (rc) return rc;
   LAUNCH(k_adj_bc, dim3(adjbc_blocks(s)), dim3(256), s->nsrc, (const int*)s->gmap, (const double*)s->b,
-         (const double*)T.Bp[0], (const double*)T.Bp[1], (const double*)T.Bp[2], s->flv, s->o.min_depth, s->eps4,
+         (const double*)T.Bp[0], (const double*)T.Bp[1], (const double*)T.Bp[2],
+         (const double*)(s->rec + (size_t)STEP_REC * k + 1), s->o.min_depth, s->eps4,
          s->lb, lB[0], lB[1], lB[2]);
   // dryClean and B = W1 + dt R1 backwards: lW1 += lB, lR1 = dt lB
   LAUNCH(k_adj_tail1, dim3(gb), dim3(256), s->W, s->H, s->o.min_depth, dt, (const double*)T.hB,
@@ -935,7 +956,8 @@ int reverse_step(swe_adjoint* s, int k, const Tape& T) {
   rc = residual_adjoint(s, T.W1, T.it1, T.th1, dt, lA);
   if (rc) return rc;
   LAUNCH(k_adj_bc, dim3(adjbc_blocks(s)), dim3(256), s->nsrc, (const int*)s->gmap, (const double*)s->b,
-         (const double*)T.W1[0], (const double*)T.W1[1], (const double*)T.W1[2], s->flv, s->o.min_depth, s->eps4,
+         (const double*)T.W1[0], (const double*)T.W1[1], (const double*)T.W1[2],
+         (const double*)(s->rec + (size_t)STEP_REC * k + 1), s->o.min_depth, s->eps4,
          s->lb, lA[0], lA[1], lA[2]);
   CU(cudaGetLastError());
   return SWE_OK;
@@ -1047,6 +1069,7 @@ int swe_adjoint_create(const swe_options* o, const double* b, const double* eta0
   s->ckpt = A(3 * N * (size_t)s->nseg);
   s->tape = nullptr;               // allocated by the first backward pass
   s->dts = A(steps);
+  s->rec = A((size_t)STEP_REC * steps);
   s->obs = A((size_t)steps * n_gauges);
   s->eta_series = A((size_t)steps * n_gauges);
   s->J = A(1);
@@ -1143,7 +1166,7 @@ int swe_adjoint_forward(swe_adjoint* s, double* J, double* gauge_eta) {
   if (!s) return fail(SWE_EINVAL, "null argument");
   const int gb = G1(s);
   k_init_state<<<gb, 256, 0, s->st>>>(s->N, s->b, s->eta0, s->A[0], s->A[1], s->A[2]);
-  CU(cudaMemsetAsync(s->ctl, 0, sizeof(Control), s->st));
+  CU(cudaMemcpyAsync(s->ctl, &s->ctl_init, sizeof(Control), cudaMemcpyHostToDevice, s->st));   // t = 0, tide tables
   CU(cudaMemsetAsync(s->J, 0, sizeof(double), s->st));
   {
     StageArgs a = stage_args(s, s->A, nullptr);
@@ -1235,6 +1258,7 @@ int swe_adjoint_set_boundary(swe_adjoint* s, int side, int kind) {
   if (side < 0 || side > 3 || kind < SWE_BC_REFLECT || kind > SWE_BC_FLATHER)
     return fail(SWE_EINVAL, "swe_adjoint_set_boundary: side 0..3 (W, E, S, N), kind reflect/outflow/periodic/flather");
   s->kind[side] = kind;
+  if (kind != SWE_BC_FLATHER) s->fl_kind[side] = 0;
   s->forward_done = false;
   return build_ghost_map(s);
 }
@@ -1242,8 +1266,26 @@ int swe_adjoint_set_boundary(swe_adjoint* s, int side, int kind) {
 int swe_adjoint_set_flather_values(swe_adjoint* s, int side, double eta_ext, double u_ext) {
   if (!s) return fail(SWE_EINVAL, "null argument");
   if (side < 0 || side > 3) return fail(SWE_EINVAL, "swe_adjoint_set_flather_values: side 0..3 (W, E, S, N)");
-  s->flv.eta[side] = eta_ext;
-  s->flv.u[side] = u_ext;
+  s->fl_eta[side] = eta_ext;
+  s->fl_u[side] = u_ext;
+  s->fl_kind[side] = 0;
+  s->kind[side] = SWE_BC_FLATHER;
+  s->forward_done = false;
+  return build_ghost_map(s);
+}
+
+int swe_adjoint_set_flather_tide(swe_adjoint* s, int side, double msl, int n, const double* amp, const double* omega,
+                                 const double* phase_deg, double u_coef) {
+  if (!s) return fail(SWE_EINVAL, "null argument");
+  if (side < 0 || side > 3) return fail(SWE_EINVAL, "swe_adjoint_set_flather_tide: side 0..3 (W, E, S, N)");
+  if (n < 0 || n > swe::MAX_TIDE) return fail(SWE_EINVAL, "tide tables hold at most 16 constituents");
+  if (n > 0 && (!amp || !omega || !phase_deg)) return fail(SWE_EINVAL, "null tide table");
+  Control& c = s->ctl_init;
+  c.tide_n[side] = n; c.tide_msl[side] = msl; c.tide_ucoef[side] = u_coef;
+  for (int q = 0; q < n; q++) {
+    c.tide_amp[side][q] = amp[q]; c.tide_omega[side][q] = omega[q]; c.tide_phase[side][q] = phase_deg[q];
+  }
+  s->fl_kind[side] = 1;
   s->kind[side] = SWE_BC_FLATHER;
   s->forward_done = false;
   return build_ghost_map(s);
