@@ -458,10 +458,17 @@ int enqueue_step(swe_sim* s, int mode, double dt, double t_end, const double* dt
   return launch_stage<2>(s, a2, pdl);
 }
 
+// Blocks of a grid-stride reduction over `cells` cells: one per 256 cells,
+// at most 2368 (16 per SM of a B200), so that the last block's ticket is
+// shared by a few thousand blocks and each thread strides over several cells.
+int reduction_blocks(const swe_sim* s, int cells) {
+  return std::min(s->part_cap, std::min(16 * 148, std::max(1, (cells + 255) / 256)));
+}
+
 int ensure_cfl(swe_sim* s) {
   if (s->cfl_valid) return SWE_OK;
   swe::StageArgs a = stage_args(s, s->d_A, nullptr);
-  const int nb = std::min(s->part_cap, std::max(1, (s->nx * s->ny + 255) / 256));
+  const int nb = reduction_blocks(s, s->nx * s->ny);
   swe::k_cfl_rate<<<nb, swe::BX, 0, s->st>>>(a, s->d_ctl, s->d_part);
   CU(cudaGetLastError());
   s->cfl_valid = true;
@@ -1140,7 +1147,7 @@ int swe_eta_projection(swe_sim* s, const double* coef, double* out) {
 static int max_diag(swe_sim* s, int what, double ref, double* out) {
   swe::StageArgs a = stage_args(s, s->d_A, nullptr);
   const int total = what == 2 ? s->N : s->nx * s->ny;
-  const int nb = std::min(s->part_cap, std::max(1, (total + 255) / 256));
+  const int nb = reduction_blocks(s, total);
   swe::k_max_diag<<<nb, swe::BX, 0, s->st>>>(a, what, ref, s->d_part, s->d_ctl);
   CU(cudaGetLastError());
   return finish_diag(s, out);

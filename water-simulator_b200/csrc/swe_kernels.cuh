@@ -698,6 +698,27 @@ __global__ void __launch_bounds__(BX, SWE_STAGE_MIN_BLOCKS) k_stage(StageArgs a,
 // ---------------------------------------------------------------------------
 // Reductions and diagnostics.
 
+// The last block's combine of the grid's per-block partials (a maximum, or
+// a sum of whole numbers: exact in any order) by all of its threads, at L2
+// (the other blocks wrote them); the result in thread 0.  One thread reading
+// 16 384 partials in turn took most of a 0.49 ms launch.
+__device__ __forceinline__ double combine_parts(const double* part, int n, bool sum, double* s_red) {
+  double mm = 0;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const double x = __ldcg(part + q);
+    mm = sum ? mm + x : fmax(mm, x);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double x = __shfl_down_sync(0xffffffffu, mm, o);
+    mm = sum ? mm + x : fmax(mm, x);
+  }
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = mm;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < (int)blockDim.x / 32; w++) mm = sum ? mm + s_red[w] : fmax(mm, s_red[w]);
+  return mm;
+}
+
 // CFL rate max over wet interior cells (src/swe.mjs:632-647) -> ctl->next_max.
 __global__ void k_cfl_rate(StageArgs a, Control* ctl, double* part) {
   __shared__ double s[BX / 32];
@@ -725,10 +746,10 @@ __global__ void k_cfl_rate(StageArgs a, Control* ctl, double* part) {
     s_last = atomicAdd(&ctl->counter, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
-    __threadfence();
-    double mm = 0;
-    for (int q = 0; q < (int)gridDim.x; q++) mm = fmax(mm, ((volatile double*)part)[q]);
+  if (!s_last) return;                            // uniform per block
+  __threadfence();
+  const double mm = combine_parts(part, gridDim.x, false, s);
+  if (threadIdx.x == 0) {
     ctl->next_max = mm;
     ctl->counter = 0;
   }
@@ -920,13 +941,10 @@ __global__ void k_max_diag(StageArgs a, int what, double ref, double* part, Cont
     s_last = atomicAdd(&ctl->counter, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
-    __threadfence();
-    double mm = 0;
-    for (int q = 0; q < (int)gridDim.x; q++) {
-      const double x = ((volatile double*)part)[q];
-      mm = what == 2 ? mm + x : fmax(mm, x);
-    }
+  if (!s_last) return;                            // uniform per block
+  __threadfence();
+  const double mm = combine_parts(part, gridDim.x, what == 2, s);
+  if (threadIdx.x == 0) {
     ctl->diag = mm;
     ctl->counter = 0;
   }
