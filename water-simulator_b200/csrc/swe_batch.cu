@@ -405,7 +405,7 @@ __global__ void k_batch_cfl(BatchBasin* basins) {
     if (hk <= a.minDepth) continue;
     const double cc = sqrt(SWE_G * hk);
     const double den = swe::vel_den(hk, a.eps4);
-    const double u = fabs(swe::vel_num(a.hu[k], hk) / den), v = fabs(swe::vel_num(a.hv[k], hk) / den);
+    const double u = fabs(swe::qdiv(swe::vel_num(a.hu[k], hk), den)), v = fabs(swe::qdiv(swe::vel_num(a.hv[k], hk), den));
     const double sr = (u + cc) / a.m.dxRow[j] + (v + cc) / a.m.dyCFL[j];
     if (sr > m) m = sr;
   }

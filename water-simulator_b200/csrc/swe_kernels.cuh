@@ -731,7 +731,7 @@ __global__ void k_cfl_rate(StageArgs a, Control* ctl, double* part) {
     if (hk <= a.minDepth) continue;
     const double cc = sqrt(SWE_G * hk);
     const double den = vel_den(hk, a.eps4);
-    const double u = fabs(vel_num(a.hu[k], hk) / den), v = fabs(vel_num(a.hv[k], hk) / den);
+    const double u = fabs(qdiv(vel_num(a.hu[k], hk), den)), v = fabs(qdiv(vel_num(a.hv[k], hk), den));
     const double sr = (u + cc) / a.m.dxRow[j] + (v + cc) / a.m.dyCFL[j];
     if (sr > m) m = sr;
   }
@@ -838,12 +838,12 @@ __global__ void k_friction(StageArgs a, double dt) {
     if (hk <= a.minDepth) { a.ohu[k] = 0; a.ohv[k] = 0; continue; }
     if (!(n != 0 && n == n)) continue;
     const double den = vel_den(hk, a.eps4);
-    const double u = vel_num(a.ohu[k], hk) / den, v = vel_num(a.ohv[k], hk) / den;
+    const double u = qdiv(vel_num(a.ohu[k], hk), den), v = qdiv(vel_num(a.ohv[k], hk), den);
     const double speed = hypot(u, v);
     if (speed < 1e-14) continue;
     const double denom = 1 + dt * SWE_G * n * n * speed / pow43(hk);
-    a.ohu[k] = a.ohu[k] / denom;
-    a.ohv[k] = a.ohv[k] / denom;
+    a.ohu[k] = qdiv(a.ohu[k], denom);
+    a.ohv[k] = qdiv(a.ohv[k], denom);
   }
 }
 
@@ -872,7 +872,7 @@ __global__ void __launch_bounds__(32 * ROWSUM_WARPS) k_row_sums(StageArgs a, int
       else if (what == 2) term = a.b[k] + hk;
       else if (!(hk <= 0)) {
         const double den = vel_den(hk, a.eps4);
-        const double u = vel_num(a.hu[k], hk) / den, v = vel_num(a.hv[k], hk) / den;
+        const double u = qdiv(vel_num(a.hu[k], hk), den), v = qdiv(vel_num(a.hv[k], hk), den);
         term = 0.5 * hk * (u * u + v * v) + 0.5 * SWE_G * hk * (hk + 2 * a.b[k]);
       }
     }
@@ -923,7 +923,7 @@ __global__ void k_max_diag(StageArgs a, int what, double ref, double* part, Cont
     if (what == 0) d = fabs(a.b[k] + hk - ref);
     else {
       const double den = vel_den(hk, a.eps4);
-      d = hypot(vel_num(a.hu[k], hk) / den, vel_num(a.hv[k], hk) / den);
+      d = hypot(qdiv(vel_num(a.hu[k], hk), den), qdiv(vel_num(a.hv[k], hk), den));
     }
     if (d > m) m = d;
   }

@@ -163,22 +163,29 @@ __device__ __forceinline__ void split_faces_cell(const StageArgs& a, const Split
     s.U[k] = Uk;
   }
 
-  // east x face (k|k+1)
-  Face fx = {0, 0, 0, 0, 0};
-  if (gj >= 2 && gj < H - 2 && gi >= 1 && gi < W - 2) {
-    fx = face_flux(bk, hk, Uk, Vk, xsE, xsB, sm.xs[2][ly][lx], sm.xs[3][ly][lx],
-                   sm.b[cy][cx + 1], sm.h[cy][cx + 1], sm.U[cy][cx + 1], sm.V[cy][cx + 1],
-                   sm.xs[0][ly][lx + 1], sm.xs[1][ly][lx + 1], sm.xs[2][ly][lx + 1], sm.xs[3][ly][lx + 1], dry);
+  // The east x face (k|k+1), then the north y face (k|k+W; v normal, u
+  // transverse), through one copy of the face solve: a loop of two passes
+  // that is not unrolled, so that the solve, the bulk of the kernel's code,
+  // sits in the instruction cache once.
+  constexpr int XS = SPY * (SPX + 1), YS = (SPY + 1) * SPX;   // strides of xs[q], ys[q]
+#pragma unroll 1
+  for (int d = 0; d < 2; d++) {
+    const bool on = d == 0 ? (gj >= 2 && gj < H - 2 && gi >= 1 && gi < W - 2)
+                           : (gj >= 1 && gj < H - 2 && gi >= 2 && gi < W - 2);
+    const double* sp = d == 0 ? &sm.xs[0][ly][lx] : &sm.ys[0][ly][lx];
+    const int fs = d == 0 ? XS : YS, no = d == 0 ? 1 : SPX;       // field stride, the neighbour's offset
+    const int qn = d == 0 ? 2 : 3, qt = 5 - qn;                  // normal and transverse velocity slopes
+    const int ry = d == 0 ? cy : cy + 1, rx = d == 0 ? cx + 1 : cx;
+    Face f = {0, 0, 0, 0, 0};
+    if (on) {
+      f = face_flux(bk, hk, d == 0 ? Uk : Vk, d == 0 ? Vk : Uk, sp[0], sp[fs], sp[qn * fs], sp[qt * fs],
+                    sm.b[ry][rx], sm.h[ry][rx], d == 0 ? sm.U[ry][rx] : sm.V[ry][rx],
+                    d == 0 ? sm.V[ry][rx] : sm.U[ry][rx],
+                    sp[no], sp[fs + no], sp[qn * fs + no], sp[qt * fs + no], dry);
+    }
+    double* const* o = d == 0 ? s.fx : s.fy;
+    o[F_M][k] = f.M; o[F_T][k] = f.T; o[F_NPL][k] = f.N + f.pL; o[F_NPR][k] = f.N + f.pR;
   }
-  s.fx[F_M][k] = fx.M; s.fx[F_T][k] = fx.T; s.fx[F_NPL][k] = fx.N + fx.pL; s.fx[F_NPR][k] = fx.N + fx.pR;
-  // north y face (k|k+W): v is normal, u transverse
-  Face fy = {0, 0, 0, 0, 0};
-  if (gj >= 1 && gj < H - 2 && gi >= 2 && gi < W - 2) {
-    fy = face_flux(bk, hk, Vk, Uk, nsE, nsB, sm.ys[3][ly][lx], sm.ys[2][ly][lx],
-                   sm.b[cy + 1][cx], sm.h[cy + 1][cx], sm.V[cy + 1][cx], sm.U[cy + 1][cx],
-                   sm.ys[0][ly + 1][lx], sm.ys[1][ly + 1][lx], sm.ys[3][ly + 1][lx], sm.ys[2][ly + 1][lx], dry);
-  }
-  s.fy[F_M][k] = fy.M; s.fy[F_T][k] = fy.T; s.fy[F_NPL][k] = fy.N + fy.pL; s.fy[F_NPR][k] = fy.N + fy.pR;
 }
 
 __device__ __forceinline__ void split_faces_finish(const StageArgs& a, const SplitBufs& s, int tx, int ty,
