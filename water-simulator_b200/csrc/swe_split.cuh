@@ -415,8 +415,11 @@ __device__ __forceinline__ void split_faces_tile_tma(const StageArgs& a, const S
   split_faces_finish(a, s, tx, ty, sm, t);
 }
 
+// 5 CTAs per SM (48 registers, 168 / 216 bytes of spills) measured +1.8% on
+// the beach over 4 (64 registers) and the same all-wet; 6 (40 registers)
+// +1.2% on the beach.
 #ifndef SWE_SPLIT_FACES_MIN_BLOCKS
-#define SWE_SPLIT_FACES_MIN_BLOCKS 4
+#define SWE_SPLIT_FACES_MIN_BLOCKS 5
 #endif
 __global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_FACES_MIN_BLOCKS)
 k_split_faces(StageArgs a, SplitBufs s, Control* ctl) {
