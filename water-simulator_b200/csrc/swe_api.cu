@@ -372,7 +372,8 @@ void make_cell_maps(swe_sim* s) {
               encode_field(encode, s, &c.m[swe::CM_H], st == 0 ? s->d_A[0] : s->d_B[0], SPX + 4, SPY + 2);
     for (int q = 0; q < 3 && ok; q++)
       ok = encode_field(encode, s, &c.m[swe::CM_XT + q], s->sb.fx[q + 1], SPX + 2, SPY) &&
-           encode_field(encode, s, &c.m[swe::CM_YT + q], s->sb.fy[q + 1], SPX, SPY + 1);
+           encode_field(encode, s, &c.m[swe::CM_YT + q], s->sb.fy[q + 1], SPX, SPY + 1) &&
+           encode_field(encode, s, &c.m[swe::CM_TB + q], s->sb.tb[q], SPX, SPY);
     if (!ok) return;
   }
   s->cell_tma = 1;

@@ -454,20 +454,22 @@ struct CellsSmem {
 // The cell kernel's inputs from the face kernel, staged by tensor-map copies
 // for the tile at (i0, j0) (TMA variant): the mass fluxes of every face the
 // limiter ring and the gather touch, the other face values of the gather and
-// the depths of the ring.  x = i0 - 2 (even) for every box but yt's; cells
-// outside the grid read as zeros, which the dry flags replace in any case.
+// the depths of the ring, and the tile's source terms.  x = i0 - 2 (even)
+// for every box but yt's and tb's (x = i0); cells outside the grid read as
+// zeros, which the dry flags replace in any case.
 struct CellFaceTiles {
   alignas(128) double xm[SPY + 2][SPX + 4];      // fx M, rows j0-1.., columns i0-2..
   alignas(128) double ym[SPY + 3][SPX + 4];      // fy M, rows j0-2.., columns i0-2..
   alignas(128) double hr[SPY + 2][SPX + 4];      // h of the stage input, rows j0-1.., columns i0-2..
   alignas(128) double xt[3][SPY][SPX + 2];       // fx T, N + pL, N + pR, rows j0.., columns i0-2..
   alignas(128) double yt[3][SPY + 1][SPX];       // fy T, N + pL, N + pR, rows j0-1.., columns i0..
+  alignas(128) double tb[3][SPY][SPX];           // the tile's bed terms x, y and geometric source
 };
-enum { CM_XM, CM_YM, CM_H, CM_XT, CM_YT = CM_XT + 3, CM_COUNT = CM_YT + 3 };
+enum { CM_XM, CM_YM, CM_H, CM_XT, CM_YT = CM_XT + 3, CM_TB = CM_YT + 3, CM_COUNT = CM_TB + 3 };
 struct CellMaps { CUtensorMap m[CM_COUNT]; };
 constexpr unsigned CELL_TX_BYTES = sizeof(double) * (unsigned)((SPY + 2) * (SPX + 4) + (SPY + 3) * (SPX + 4) +
                                                                (SPY + 2) * (SPX + 4) + 3 * SPY * (SPX + 2) +
-                                                               3 * (SPY + 1) * SPX);
+                                                               3 * (SPY + 1) * SPX + 3 * SPY * SPX);
 
 // A face / source-term value owned by cell (gi, gj) of the 3 x 3 tile
 // neighbourhood of the tile at (i0, j0): +0 when its tile was dry.
@@ -627,7 +629,10 @@ __device__ __forceinline__ void split_cell(const StageArgs& a, const SplitBufs& 
   cp_async_wait_all();
   const double hin = sm.st[0][t], huin = sm.st[1][t], hvin = sm.st[2][t];
   double tb0 = 0, tb1 = 0, tg = 0, Uk = 0;
-  if (!DRY && interior && bedOn && !dC) { tb0 = s.tb[0][k]; tb1 = s.tb[1][k]; if (sph) tg = s.tb[2][k]; }
+  if (!DRY && interior && bedOn && !dC) {
+    if (ST) { tb0 = ft->tb[0][ly][lx]; tb1 = ft->tb[1][ly][lx]; if (sph) tg = ft->tb[2][ly][lx]; }
+    else { tb0 = s.tb[0][k]; tb1 = s.tb[1][k]; if (sph) tg = s.tb[2][k]; }
+  }
   if (interior && sph) {
     if (!DRY && !dC) Uk = s.U[k];
     else Uk = vel_num(huin, hin);               // h is 0 here: the face kernel's u
@@ -848,6 +853,7 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
       for (int q = 0; q < 3; q++) {
         tma_load_tile(&ft->xt[q][0][0], &maps->m[CM_XT + q], x, j0, bar);
         tma_load_tile(&ft->yt[q][0][0], &maps->m[CM_YT + q], i0, j0 - 1, bar);
+        tma_load_tile(&ft->tb[q][0][0], &maps->m[CM_TB + q], i0, j0, bar);
       }
     }
     const bool ok = mbar_wait_bounded(bar, 0, TMA_WAIT_TRIES);
