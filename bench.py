@@ -594,11 +594,11 @@ def fma_build_summary(steps, warmup):
 
 def launches_per_step(swe, lib, sim):
     """Kernel launches of one step: prepare, two ghost fills and two stages
-    of the stage kernels in use (the tiled pair and its close, or the fused
-    kernel)."""
+    of the stage kernels in use (the tiled pair per stage and one close of
+    the step, or the fused kernel per stage)."""
     impl = ctypes.c_int(-1)
     swe._lib.check(lib.swe_get_stage_kernels(sim._h, ctypes.byref(impl)))
-    return 3 + 2 * (3 if impl.value == 1 else 1)
+    return 3 + (5 if impl.value == 1 else 2)
 
 
 def launch_cfg(swe, lib, sim):

@@ -430,8 +430,10 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
     } else {
       CU(launch(pdl, swe::k_split_cells<MODE, false>, s->sgrid, blk, s->st, a, sb, s->d_ctl));
     }
-    CU(launch(pdl, swe::k_split_close_multi<MODE>, dim3(swe::CLOSE_BLOCKS), blk, s->st, a, s->d_ctl,
-              (int)(s->sgrid.x * s->sgrid.y), s->d_part + 3 * (size_t)s->part_cap));
+    // stage 2's close closes the whole step, stage 1's floored mass included
+    if (MODE == 2)
+      CU(launch(pdl, swe::k_split_close_multi<2>, dim3(swe::CLOSE_BLOCKS), blk, s->st, a, s->d_ctl,
+                (int)(s->sgrid.x * s->sgrid.y), s->d_part + 3 * (size_t)s->part_cap));
   } else {
     swe::k_stage<MODE><<<s->grid, swe::BX, swe::STAGE_SMEM_BYTES, s->st>>>(a, s->d_ctl);
   }
@@ -634,11 +636,11 @@ int swe_create(const swe_options* o, const double* b, const double* h, swe_sim**
   CUB(cudaMalloc(&s->d_b, nb));
   for (int q = 0; q < 3; q++) { CUB(cudaMalloc(&s->d_A[q], nb)); CUB(cudaMalloc(&s->d_B[q], nb)); }
   CUB(cudaMalloc(&s->d_geom, sizeof(double) * (SWE_GEOM_NROWS + 3) * s->H));
-  CUB(cudaMalloc(&s->d_part, sizeof(double) * (3 * s->part_cap + 2 * swe::CLOSE_BLOCKS)));   // + the close's scratch
+  CUB(cudaMalloc(&s->d_part, sizeof(double) * (3 * s->part_cap + 3 * swe::CLOSE_BLOCKS)));   // + the close's scratch
   CUB(cudaMalloc(&s->d_rows, sizeof(double) * std::max(1, s->ny)));
   CUB(cudaMalloc(&s->d_ctl, sizeof(swe::Control)));
   CUB(cudaMemsetAsync(s->d_ctl, 0, sizeof(swe::Control), s->st));
-  CUB(cudaMemsetAsync(s->d_part, 0, sizeof(double) * (3 * s->part_cap + 2 * swe::CLOSE_BLOCKS), s->st));
+  CUB(cudaMemsetAsync(s->d_part, 0, sizeof(double) * (3 * s->part_cap + 3 * swe::CLOSE_BLOCKS), s->st));
   for (int q = 0; q < 3; q++) {
     CUB(cudaMemsetAsync(s->d_A[q], 0, nb, s->st));
     CUB(cudaMemsetAsync(s->d_B[q], 0, nb, s->st));

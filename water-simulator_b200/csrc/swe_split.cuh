@@ -938,35 +938,43 @@ k_split_cells(StageArgs a, SplitBufs s, Control* ctl) {
 // and closes the stage as split_close_block does.  The maximum is the same
 // in any order; the floored mass is summed in this fixed order.  One block
 // reading 16 705 slots spent most of its time in dependent rounds of L2
-// loads.  scratch holds 2 * CLOSE_BLOCKS doubles.
+// loads.  MODE 2 closes the whole step: stage 1's floored mass is needed
+// only there, so it is summed here too (the same order as MODE 1 sums it)
+// and stage 1 needs no close of its own.  scratch holds 3 * CLOSE_BLOCKS
+// doubles.
 constexpr int CLOSE_BLOCKS = 32;
 template <int MODE>
 __global__ void __launch_bounds__(SP_THREADS) k_split_close_multi(StageArgs a, Control* ctl, int nparts,
                                                                     double* scratch) {
   pdl_enter();
   if (ctl->stop) return;
-  __shared__ double red[2][SP_THREADS / 32];
+  __shared__ double red[3][SP_THREADS / 32];
   __shared__ int last;
   const int t = threadIdx.x, b = blockIdx.x;
   const int chunk = (nparts + CLOSE_BLOCKS - 1) / CLOSE_BLOCKS;
   const int q0 = b * chunk, q1 = min(nparts, q0 + chunk);
   const double* pf = MODE == 1 ? a.part_fl1 : a.part_fl2;
-  double m = 0, f = 0;
+  double m = 0, f = 0, f1 = 0;
   for (int q = q0 + t; q < q1; q += SP_THREADS) {
-    if (MODE == 2) m = fmax(m, __ldcg(a.part_max + q));
+    if (MODE == 2) {
+      m = fmax(m, __ldcg(a.part_max + q));
+      f1 += __ldcg(a.part_fl1 + q);
+    }
     f += __ldcg(pf + q);
   }
   for (int o = 16; o > 0; o >>= 1) {
     m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
     f += __shfl_down_sync(0xffffffffu, f, o);
+    f1 += __shfl_down_sync(0xffffffffu, f1, o);
   }
-  if ((t & 31) == 0) { red[0][t >> 5] = m; red[1][t >> 5] = f; }
+  if ((t & 31) == 0) { red[0][t >> 5] = m; red[1][t >> 5] = f; red[2][t >> 5] = f1; }
   __syncthreads();
   if (t == 0) {
-    m = red[0][0]; f = red[1][0];
-    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, red[0][w]); f += red[1][w]; }
+    m = red[0][0]; f = red[1][0]; f1 = red[2][0];
+    for (int w = 1; w < SP_THREADS / 32; w++) { m = fmax(m, red[0][w]); f += red[1][w]; f1 += red[2][w]; }
     scratch[b] = m;
     scratch[CLOSE_BLOCKS + b] = f;
+    scratch[2 * CLOSE_BLOCKS + b] = f1;
     __threadfence();
     last = atomicAdd(&ctl->counter, 1u) == (unsigned int)(CLOSE_BLOCKS - 1);
   }
@@ -976,17 +984,20 @@ __global__ void __launch_bounds__(SP_THREADS) k_split_close_multi(StageArgs a, C
   static_assert(CLOSE_BLOCKS == 32, "one block result per lane");
   m = __ldcg(scratch + t);
   f = __ldcg(scratch + CLOSE_BLOCKS + t);
+  f1 = __ldcg(scratch + 2 * CLOSE_BLOCKS + t);
   for (int o = 16; o > 0; o >>= 1) {
     m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
     f += __shfl_down_sync(0xffffffffu, f, o);
+    f1 += __shfl_down_sync(0xffffffffu, f1, o);
   }
   if (t == 0) {
     const double dt = ctl->dt;
     if (MODE == 1) {
       ctl->floored1 = f;
     } else {
+      ctl->floored1 = f1;
       ctl->next_max = m;
-      ctl->mass_floored = ctl->floored1 + f;
+      ctl->mass_floored = f1 + f;
       ctl->t = ctl->t + dt;
       ctl->steps = ctl->steps + 1;
     }
