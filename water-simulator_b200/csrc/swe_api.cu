@@ -319,11 +319,6 @@ int launch_bc(swe_sim* s, double* const* f, int respect_stop, bool pdl = false) 
   return SWE_OK;
 }
 
-// Tensor maps of the face kernel's state tile (swe_split.cuh, TileMaps):
-// b, h, hu, hv of A (stage 1's input) and of B (stage 2's), each a 2-D
-// W x H array of doubles, box SSXT x SSY, zeros outside.  A row stride that
-// is not a multiple of 16 bytes (odd W), a driver without the encoder, or
-// SWE_B200_TMA=0 leaves the per-element copies in use (the same bits).
 // The driver's tensor-map encoder, or null; and whether the tile copies are
 // on for this grid (SWE_B200_TMA=0 turns them off; a row stride that is not
 // a multiple of 16 bytes cannot take them).
@@ -379,6 +374,11 @@ void make_cell_maps(swe_sim* s) {
   s->cell_tma = 1;
 }
 
+// Tensor maps of the face kernel's state tile (swe_split.cuh, TileMaps):
+// b, h, hu, hv of A (stage 1's input) and of B (stage 2's), each a 2-D
+// W x H array of doubles, box SSXT x SSY, zeros outside.  A row stride that
+// is not a multiple of 16 bytes (odd W), a driver without the encoder, or
+// SWE_B200_TMA=0 leaves the per-element copies in use (the same bits).
 void make_tile_maps(swe_sim* s) {
   s->tma = 0;
   if (!tma_wanted(s)) return;
