@@ -289,7 +289,13 @@ __device__ __forceinline__ void split_faces_finish_l(const StageArgs& a, const S
   if (allDry) return;                           // uniform across the CTA
   // velocities over the whole box; a cell outside the grid has h = hu =
   // hv = 0 there and gets u = v = +0, as it would have kept
-  for (int q = t; q < SSXT * SSY; q += SP_THREADS) {
+  // The box has more cells than the CTA has threads: the second pass goes
+  // to the last threads, since the first two warps take the extra slopes.
+  constexpr int VREM = SSXT * SSY - SP_THREADS;
+  static_assert(VREM > 0 && VREM <= SP_THREADS, "one or two box cells per thread");
+  for (int pass = 0; pass < 2; pass++) {
+    if (pass == 1 && t < SP_THREADS - VREM) break;
+    const int q = pass == 0 ? t : t + VREM;
     const int ly = q / SSXT, c = q - ly * SSXT;
     const double h = sm.h[ly][c], hu = sm.U[ly][c], hv = sm.V[ly][c];
     double U, V;
@@ -415,13 +421,19 @@ __device__ __forceinline__ void split_faces_tile_tma(const StageArgs& a, const S
   split_faces_finish(a, s, tx, ty, sm, t);
 }
 
-// 5 CTAs per SM (48 registers, 168 / 216 bytes of spills) measured +1.8% on
-// the beach over 4 (64 registers) and the same all-wet; 6 (40 registers)
-// +1.2% on the beach.
+// CTAs per SM of the face kernels.  The tensor-map kernel of the stepping
+// loop at 5 (48 registers, 168 / 216 bytes of spills) measured +1.8% on the
+// beach over 4 (64 registers) and the same all-wet; 6 (40 registers) +1.2%.
+// The per-element kernel, which the adjoint's passes use (they also write
+// the slopes and velocities to the tape), stays at 4: at 5 its gradient cost
+// 2% more against an unchanged forward.
 #ifndef SWE_SPLIT_FACES_MIN_BLOCKS
 #define SWE_SPLIT_FACES_MIN_BLOCKS 5
 #endif
-__global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_FACES_MIN_BLOCKS)
+#ifndef SWE_SPLIT_FACES_PLAIN_MIN_BLOCKS
+#define SWE_SPLIT_FACES_PLAIN_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_FACES_PLAIN_MIN_BLOCKS)
 k_split_faces(StageArgs a, SplitBufs s, Control* ctl) {
   pdl_enter();
   if (ctl->stop) return;
@@ -866,7 +878,12 @@ __device__ __forceinline__ void split_cells_tile(const StageArgs& a, const Split
     }
   }
   if (!fold) {
-    for (int q = t; q < (SPX + 2) * (SPY + 2); q += SP_THREADS) {
+    // the ring's second pass on the last threads, as the velocities'
+    constexpr int TREM = (SPX + 2) * (SPY + 2) - SP_THREADS;
+    static_assert(TREM > 0 && TREM <= SP_THREADS, "one or two ring cells per thread");
+    for (int pass = 0; pass < 2; pass++) {
+      if (pass == 1 && t < SP_THREADS - TREM) break;
+      const int q = pass == 0 ? t : t + TREM;
       const int ly = q / (SPX + 2), lx = q - ly * (SPX + 2);
       if (TMA) sm.th[ly][lx] = allDry ? 1.0 : split_theta_st(a, *ft, sm, i0, j0, dt, i0 - 1 + lx, j0 - 1 + ly);
       else sm.th[ly][lx] = allDry ? 1.0 : split_theta(a, s, sm, i0, j0, dt, i0 - 1 + lx, j0 - 1 + ly);
