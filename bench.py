@@ -598,7 +598,14 @@ def launches_per_step(swe, lib, sim):
     the step, or the fused kernel per stage)."""
     impl = ctypes.c_int(-1)
     swe._lib.check(lib.swe_get_stage_kernels(sim._h, ctypes.byref(impl)))
-    return 3 + (5 if impl.value == 1 else 2)
+    if impl.value != 1:
+        return 3 + 2
+    # with tensor-map tiles (an even padded width) each face kernel is led by
+    # the kernel that lists the tiles it must compute
+    dims = (ctypes.c_int * 4)()
+    swe._lib.check(lib.swe_get_dims(sim._h, dims))
+    listed = dims[0] % 2 == 0 and os.environ.get("SWE_B200_TMA") != "0" and os.environ.get("SWE_B200_FACE_LIST") != "0"
+    return 3 + 5 + (2 if listed else 0)
 
 
 def launch_cfg(swe, lib, sim):

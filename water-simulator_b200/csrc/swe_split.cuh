@@ -397,9 +397,10 @@ constexpr int TMA_WAIT_TRIES = 1 << 22;
 // sets bit 4 of Control::status and leaves the tile's faces unwritten.
 __device__ __forceinline__ void split_faces_tile_tma(const StageArgs& a, const SplitBufs& s, int tx, int ty,
                                                      FacesSmem& sm, const TileMaps& maps,
-                                                     unsigned long long* bar, unsigned& parity, Control* ctl) {
+                                                     unsigned long long* bar, unsigned& parity, Control* ctl,
+                                                     bool check_settled = true) {
   const int t = threadIdx.x;
-  if (split_faces_settled(s, tx, ty, t)) return;
+  if (check_settled && split_faces_settled(s, tx, ty, t)) return;
   if (t == 0) {
     // the generic-proxy accesses of a previous tile come before the copy's writes
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -452,6 +453,67 @@ k_split_faces_tma(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant_
   __syncthreads();
   unsigned parity = 0;
   split_faces_tile_tma(a, s, blockIdx.x, blockIdx.y, sm, maps, &bar, parity, ctl);
+}
+
+// ---- the face kernel over a list of the tiles it must compute ----------------
+// On wet/dry grids most tiles settle: their 3 x 3 neighbourhood is recorded
+// dry, and the face kernel only writes their dry flag.  A CTA per tile then
+// spends much of the launch on CTAs that read nine flags and exit.
+// k_face_list does that test for every tile (one thread each), writes the
+// dry flag of the settled ones itself, and appends the others to a list
+// that the face kernel's first CTAs take.  The
+// list's order depends on timing, the results do not: every tile writes
+// only its own faces, terms and flag.  count is this stage's counter (the
+// list kernel of the other stage zeroes it again, after its face kernel
+// has run).
+__global__ void __launch_bounds__(256) k_face_list(SplitBufs s, int* list, int* count, int* other_count) {
+  pdl_enter();
+  __shared__ int wbase[8], base;
+  const int t = threadIdx.x, ntiles = s.ntx * s.nty;
+  const int tile = blockIdx.x * blockDim.x + t;
+  bool active = false;
+  if (tile < ntiles) {
+    const int tx = tile % s.ntx, ty = tile / s.ntx;
+    bool settled = true;
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) {
+        const int txn = tx - 1 + c, tyn = ty - 1 + r;
+        if (txn >= 0 && txn < s.ntx && tyn >= 0 && tyn < s.nty && !s.odry_in[tyn * s.ntx + txn]) settled = false;
+      }
+    if (settled) s.dry[tile] = 1;
+    active = !settled;
+  }
+  if (blockIdx.x == 0 && t == 0) *other_count = 0;
+  const unsigned m = __ballot_sync(0xffffffffu, active);
+  const int w = t >> 5, lane = t & 31;
+  if (lane == 0) wbase[w] = __popc(m);
+  __syncthreads();
+  if (t == 0) {
+    int n = 0;
+    for (int q = 0; q < 8; q++) { const int c = wbase[q]; wbase[q] = n; n += c; }
+    base = n ? atomicAdd(count, n) : 0;
+  }
+  __syncthreads();
+  if (active) {
+    const int at = base + wbase[w] + __popc(m & ((1u << lane) - 1));
+    if (at < ntiles) list[at] = tile;            // always, while each stage's counter is reset in turn
+  }
+}
+
+// The face kernel over the list: CTA b computes the list's entry b, and the
+// CTAs past the list's length exit after reading it.
+__global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_FACES_MIN_BLOCKS)
+k_split_faces_tma_list(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant__ TileMaps maps,
+                       const int* list, const int* count) {
+  __shared__ FacesSmem sm;
+  __shared__ alignas(8) unsigned long long bar;
+  pdl_enter();
+  if ((int)blockIdx.x >= min(*count, s.ntx * s.nty) || ctl->stop) return;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  const int tile = list[blockIdx.x];
+  unsigned parity = 0;
+  split_faces_tile_tma(a, s, tile % s.ntx, tile / s.ntx, sm, maps, &bar, parity, ctl, false);
 }
 
 struct CellsSmem {
