@@ -103,8 +103,9 @@ struct swe_sim {
   int cell_tma = 0;                                // 1: they are in use
   int* d_flist = nullptr;                          // the face kernel's tile list and its two counters
   int* d_fcount = nullptr;
-  int face_list = 0;                               // 1: the face kernel walks the list
-  int face_list_ctas = 0;                          // its resident grid
+  int* d_clist = nullptr;                          // the cell kernel's tile list and its two counters
+  int* d_ccount = nullptr;
+  int face_list = 0;                               // 1: the face kernel takes the list
   swe::SplitBufs sb;
   dim3 sgrid;
   // Whether the tiled cell kernels may settle dry tiles (swe_split.cuh).
@@ -401,8 +402,9 @@ int ensure_split(swe_sim* s) {
   if (s->d_split) return SWE_OK;
   const size_t N = s->N;
   const size_t ntiles = (size_t)s->sgrid.x * s->sgrid.y;
-  // + three int flags per tile, the face kernel's tile list and its two counters
-  const size_t doubles = swe::SPLIT_FIELDS * N + 3 * ((ntiles + 1) / 2) + (ntiles + 3) / 2;
+  // + three int flags per tile, and the face and cell kernels' tile lists
+  // with two counters each
+  const size_t doubles = swe::SPLIT_FIELDS * N + 3 * ((ntiles + 1) / 2) + (ntiles + 2);
   CU(cudaMalloc(&s->d_split, sizeof(double) * doubles));
   CU(cudaMemsetAsync(s->d_split, 0, sizeof(double) * doubles, s->st));
   s->sb = swe::split_bufs_at(s->d_split, N);
@@ -412,25 +414,15 @@ int ensure_split(swe_sim* s) {
   s->d_odry[0] = reinterpret_cast<int*>(s->d_split + swe::SPLIT_FIELDS * N + (ntiles + 1) / 2);
   s->d_odry[1] = reinterpret_cast<int*>(s->d_split + swe::SPLIT_FIELDS * N + 2 * ((ntiles + 1) / 2));
   s->d_flist = reinterpret_cast<int*>(s->d_split + swe::SPLIT_FIELDS * N + 3 * ((ntiles + 1) / 2));
-  s->d_fcount = s->d_flist + ntiles;
+  s->d_fcount = s->d_flist + ntiles;                // [2]
+  s->d_clist = s->d_fcount + 2;
+  s->d_ccount = s->d_clist + ntiles;               // [2]
   make_cell_maps(s);
-  // The face kernel over a tile list (swe_split.cuh, k_face_list): with the
-  // tensor-map copies, on a grid of resident CTAs; SWE_B200_FACE_LIST=0
-  // keeps one CTA per tile (the same bits).
-  s->face_list = 0;
+  // The face kernel led by a tile list (swe_split.cuh, k_face_list), with
+  // the tensor-map copies; SWE_B200_FACE_LIST=0 keeps every CTA testing its
+  // own tile (the same bits).
   const char* fl = std::getenv("SWE_B200_FACE_LIST");
-  if (s->tma && !(fl && std::strcmp(fl, "0") == 0)) {
-    int per_sm = 0, sms = 0, dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, swe::k_split_faces_tma_list, swe::SP_THREADS, 0) ==
-            cudaSuccess &&
-        per_sm > 0 && sms > 0) {
-      s->face_list_ctas = (int)std::min<size_t>(ntiles, (size_t)per_sm * sms);
-      s->face_list = 1;
-    }
-    cudaGetLastError();
-  }
+  s->face_list = s->tma && !(fl && std::strcmp(fl, "0") == 0) ? 1 : 0;
   return SWE_OK;
 }
 
@@ -443,17 +435,31 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
     sb.odry_in = s->d_odry[MODE == 1 ? 0 : 1];
     sb.odry_out = s->d_odry[MODE == 1 ? 1 : 0];
     const dim3 blk(swe::SP_THREADS);
-    if (s->face_list) {
+    // The tile lists pay where tiles settle: with the settling cell kernel
+    // (which swe_run keeps only where a quarter or more of the tiles settle).
+    const bool listed = s->face_list && s->settle;
+    const int cell_list = listed && s->cell_tma && sb.odry_out && a.dryfold && a.minDepth >= 0 &&
+                          a.sponge_width <= 0 && !a.h0c && !a.tape_th && !a.tape_hpre && !a.tape_pre[0];
+    if (listed) {
       const int ntiles = (int)(s->sgrid.x * s->sgrid.y);
-      CU(launch(pdl, swe::k_face_list, dim3((ntiles + 255) / 256), dim3(256), s->st, sb, s->d_flist,
-                s->d_fcount + (MODE - 1), s->d_fcount + (2 - MODE)));
+      const int cell_skip = cell_list;
+      CU(launch(pdl, swe::k_face_list, dim3((ntiles + 255) / 256), dim3(256), s->st, sb, s->d_ctl, s->d_flist,
+                s->d_fcount + (MODE - 1), s->d_fcount + (2 - MODE), cell_skip, s->d_clist,
+                s->d_ccount + (MODE - 1), s->d_ccount + (2 - MODE), s->W, s->H));
       CU(launch(pdl, swe::k_split_faces_tma_list, dim3(ntiles), blk, s->st, a, sb, s->d_ctl,
                 s->tmaps[MODE - 1], (const int*)s->d_flist, (const int*)(s->d_fcount + (MODE - 1))));
     } else if (s->tma) {
       CU(launch(pdl, swe::k_split_faces_tma, s->sgrid, blk, s->st, a, sb, s->d_ctl, s->tmaps[MODE - 1]));
     }
     else CU(launch(pdl, swe::k_split_faces, s->sgrid, blk, s->st, a, sb, s->d_ctl));
-    if (s->cell_tma) {
+    if (cell_list) {                               // only when tiles may be left out
+      const swe::CellMaps& cm = s->cmaps[MODE - 1];
+      const int ntiles = (int)(s->sgrid.x * s->sgrid.y);
+      const int* cl = s->d_clist;
+      const int* cc = s->d_ccount + (MODE - 1);
+      if (s->settle) CU(launch(pdl, swe::k_split_cells_tma_list<MODE, true>, dim3(ntiles), blk, s->st, a, sb, s->d_ctl, cm, cl, cc));
+      else CU(launch(pdl, swe::k_split_cells_tma_list<MODE, false>, dim3(ntiles), blk, s->st, a, sb, s->d_ctl, cm, cl, cc));
+    } else if (s->cell_tma) {
       const swe::CellMaps& cm = s->cmaps[MODE - 1];
       if (s->settle) CU(launch(pdl, swe::k_split_cells_tma<MODE, true>, s->sgrid, blk, s->st, a, sb, s->d_ctl, cm));
       else CU(launch(pdl, swe::k_split_cells_tma<MODE, false>, s->sgrid, blk, s->st, a, sb, s->d_ctl, cm));

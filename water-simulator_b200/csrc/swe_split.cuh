@@ -466,38 +466,78 @@ k_split_faces_tma(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant_
 // only its own faces, terms and flag.  count is this stage's counter (the
 // list kernel of the other stage zeroes it again, after its face kernel
 // has run).
-__global__ void __launch_bounds__(256) k_face_list(SplitBufs s, int* list, int* count, int* other_count) {
-  pdl_enter();
-  __shared__ int wbase[8], base;
-  const int t = threadIdx.x, ntiles = s.ntx * s.nty;
-  const int tile = blockIdx.x * blockDim.x + t;
-  bool active = false;
-  if (tile < ntiles) {
-    const int tx = tile % s.ntx, ty = tile / s.ntx;
-    bool settled = true;
-    for (int r = 0; r < 3; r++)
-      for (int c = 0; c < 3; c++) {
-        const int txn = tx - 1 + c, tyn = ty - 1 + r;
-        if (txn >= 0 && txn < s.ntx && tyn >= 0 && tyn < s.nty && !s.odry_in[tyn * s.ntx + txn]) settled = false;
-      }
-    if (settled) s.dry[tile] = 1;
-    active = !settled;
-  }
-  if (blockIdx.x == 0 && t == 0) *other_count = 0;
-  const unsigned m = __ballot_sync(0xffffffffu, active);
-  const int w = t >> 5, lane = t & 31;
+//
+// The same kernel lists the tiles the cell kernel must run when some may be
+// left out (cell_skip: the settling cell kernel is in use and nothing it
+// takes rules settling out; otherwise the cell kernel runs every tile).
+// The cell kernel settles a ghost-free tile whose 3 x 3 dry flags are set
+// (its faces are all +0), and writes nothing but +0 and 0 partials when the
+// tile's output record already says (+0, +0, +0): record 2.  Those partial
+// slots hold +0 and 0 since that record was written, so the tile can be
+// left out altogether when every tile of its 3 x 3 neighbourhood settles in
+// the face kernel (their dry flags are then set here) and its own output
+// record is 2.  The count of settled tiles (one in 16) that the cell kernel
+// keeps is kept here for the tiles left out.
+__device__ __forceinline__ bool tile_rec_dry(const int* rec, int ntx, int nty, int tx, int ty) {
+  return tx < 0 || tx >= ntx || ty < 0 || ty >= nty || rec[ty * ntx + tx] != 0;
+}
+__device__ __forceinline__ bool tile_face_settled(const int* rec, int ntx, int nty, int tx, int ty) {
+  for (int r = -1; r <= 1; r++)
+    for (int c = -1; c <= 1; c++)
+      if (!tile_rec_dry(rec, ntx, nty, tx + c, ty + r)) return false;
+  return true;
+}
+// The warp-aggregated append of `on` lanes to list (a block base from one
+// atomic on count); every thread of the block calls it.
+__device__ __forceinline__ void block_append(bool on, int value, int* list, int* count, int cap, int* wbase,
+                                             int* base) {
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  const unsigned m = __ballot_sync(0xffffffffu, on);
   if (lane == 0) wbase[w] = __popc(m);
   __syncthreads();
   if (t == 0) {
     int n = 0;
-    for (int q = 0; q < 8; q++) { const int c = wbase[q]; wbase[q] = n; n += c; }
-    base = n ? atomicAdd(count, n) : 0;
+    for (int q = 0; q < (int)blockDim.x / 32; q++) { const int c = wbase[q]; wbase[q] = n; n += c; }
+    *base = n ? atomicAdd(count, n) : 0;
   }
   __syncthreads();
-  if (active) {
-    const int at = base + wbase[w] + __popc(m & ((1u << lane) - 1));
-    if (at < ntiles) list[at] = tile;            // always, while each stage's counter is reset in turn
+  if (on) {
+    const int at = *base + wbase[w] + __popc(m & ((1u << lane) - 1));
+    if (at < cap) list[at] = value;              // always, while each stage's counter is reset in turn
   }
+  __syncthreads();
+}
+__global__ void __launch_bounds__(256) k_face_list(SplitBufs s, Control* ctl, int* list, int* count,
+                                                   int* other_count, int cell_skip, int* clist, int* ccount,
+                                                   int* other_ccount, int W, int H) {
+  pdl_enter();
+  __shared__ int wbase[8], base;
+  const int t = threadIdx.x, ntx = s.ntx, nty = s.nty, ntiles = ntx * nty;
+  const int tile = blockIdx.x * blockDim.x + t;
+  bool faces = false, cells = false;
+  if (tile < ntiles) {
+    const int tx = tile % ntx, ty = tile / ntx;
+    const bool settled = tile_face_settled(s.odry_in, ntx, nty, tx, ty);
+    if (settled) s.dry[tile] = 1;
+    faces = !settled;
+    cells = true;
+    const double dt = ctl->dt;
+    const int i0 = tx * SPX, j0 = ty * SPY;
+    if (cell_skip && settled && dt > 0 && dt < INFINITY && i0 >= 2 && i0 + SPX <= W - 2 && j0 >= 2 &&
+        j0 + SPY <= H - 2 && s.odry_out[tile] == 2) {
+      bool all = true;
+      for (int r = -1; r <= 1 && all; r++)
+        for (int c = -1; c <= 1 && all; c++)
+          if (!(r == 0 && c == 0)) all = tile_face_settled(s.odry_in, ntx, nty, tx + c, ty + r);
+      if (all) {
+        cells = false;
+        if ((tile & 15) == 0) atomicAdd(&ctl->settled_next, 1);
+      }
+    }
+  }
+  if (blockIdx.x == 0 && t == 0) { *other_count = 0; *other_ccount = 0; }
+  block_append(faces, tile, list, count, ntiles, wbase, &base);
+  if (cell_skip) block_append(cells, tile, clist, ccount, ntiles, wbase, &base);   // uniform
 }
 
 // The face kernel over the list: CTA b computes the list's entry b, and the
@@ -1097,6 +1137,24 @@ k_split_cells_tma(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant_
   if (ctl->stop) return;
   split_cells_tile<MODE, SETTLE, true>(a, s, ctl, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
                                        gridDim.x * gridDim.y, sm, false, &ft, &maps, &bar);
+}
+
+// The cell kernel over its list: CTA b runs the list's entry b; the CTAs
+// past the list's length exit after reading it.
+template <int MODE, bool SETTLE = false>
+__global__ void __launch_bounds__(SP_THREADS, SWE_SPLIT_CELLS_MIN_BLOCKS)
+k_split_cells_tma_list(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant__ CellMaps maps,
+                       const int* list, const int* count) {
+  __shared__ CellsSmem sm;
+  __shared__ CellFaceTiles ft;
+  __shared__ alignas(8) unsigned long long bar;
+  pdl_enter();
+  const int ntiles = s.ntx * s.nty;
+  if ((int)blockIdx.x >= min(*count, ntiles) || ctl->stop) return;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  const int tile = list[blockIdx.x];
+  split_cells_tile<MODE, SETTLE, true>(a, s, ctl, tile % s.ntx, tile / s.ntx, tile, ntiles, sm, false, &ft, &maps,
+                                       &bar);
 }
 
 // Closes the stage k_split_cells left open: one block, no atomics (a
