@@ -443,7 +443,8 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
     if (listed) {
       const int ntiles = (int)(s->sgrid.x * s->sgrid.y);
       const int cell_skip = cell_list;
-      CU(launch(pdl, swe::k_face_list, dim3((ntiles + 255) / 256), dim3(256), s->st, sb, s->d_ctl, s->d_flist,
+      CU(launch(pdl, swe::k_face_list, dim3((s->sgrid.x + swe::LX - 1) / swe::LX, (s->sgrid.y + swe::LY - 1) / swe::LY),
+                dim3(swe::LX * swe::LY), s->st, sb, s->d_ctl, s->d_flist,
                 s->d_fcount + (MODE - 1), s->d_fcount + (2 - MODE), cell_skip, s->d_clist,
                 s->d_ccount + (MODE - 1), s->d_ccount + (2 - MODE), s->W, s->H));
       CU(launch(pdl, swe::k_split_faces_tma_list, dim3(ntiles), blk, s->st, a, sb, s->d_ctl,

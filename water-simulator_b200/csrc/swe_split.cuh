@@ -461,8 +461,8 @@ k_split_faces_tma(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant_
 // spends much of the launch on CTAs that read nine flags and exit.
 // k_face_list does that test for every tile (one thread each), writes the
 // dry flag of the settled ones itself, and appends the others to a list
-// that the face kernel's first CTAs take.  The
-// list's order depends on timing, the results do not: every tile writes
+// that the face kernel's first CTAs take.  The list's order depends on
+// timing, the results do not: every tile writes
 // only its own faces, terms and flag.  count is this stage's counter (the
 // list kernel of the other stage zeroes it again, after its face kernel
 // has run).
@@ -478,15 +478,6 @@ k_split_faces_tma(StageArgs a, SplitBufs s, Control* ctl, const __grid_constant_
 // the face kernel (their dry flags are then set here) and its own output
 // record is 2.  The count of settled tiles (one in 16) that the cell kernel
 // keeps is kept here for the tiles left out.
-__device__ __forceinline__ bool tile_rec_dry(const int* rec, int ntx, int nty, int tx, int ty) {
-  return tx < 0 || tx >= ntx || ty < 0 || ty >= nty || rec[ty * ntx + tx] != 0;
-}
-__device__ __forceinline__ bool tile_face_settled(const int* rec, int ntx, int nty, int tx, int ty) {
-  for (int r = -1; r <= 1; r++)
-    for (int c = -1; c <= 1; c++)
-      if (!tile_rec_dry(rec, ntx, nty, tx + c, ty + r)) return false;
-  return true;
-}
 // The warp-aggregated append of `on` lanes to list (a block base from one
 // atomic on count); every thread of the block calls it.
 __device__ __forceinline__ void block_append(bool on, int value, int* list, int* count, int cap, int* wbase,
@@ -507,17 +498,38 @@ __device__ __forceinline__ void block_append(bool on, int value, int* list, int*
   }
   __syncthreads();
 }
-__global__ void __launch_bounds__(256) k_face_list(SplitBufs s, Control* ctl, int* list, int* count,
-                                                   int* other_count, int cell_skip, int* clist, int* ccount,
-                                                   int* other_ccount, int W, int H) {
+// One CTA per 32 x 8 region of tiles: the records of the region and two
+// tiles around it go to shared memory in one coalesced pass, the settled
+// test of the region and one tile around it is made there, and each thread
+// then decides for its own tile.
+constexpr int LX = 32, LY = 8;                     // tiles per list CTA
+__global__ void __launch_bounds__(LX * LY) k_face_list(SplitBufs s, Control* ctl, int* list, int* count,
+                                                       int* other_count, int cell_skip, int* clist, int* ccount,
+                                                       int* other_ccount, int W, int H) {
   pdl_enter();
-  __shared__ int wbase[8], base;
+  __shared__ unsigned char rec[LY + 4][LX + 4];      // record dry (or outside the grid)
+  __shared__ unsigned char fs[LY + 2][LX + 2];       // settles in the face kernel
+  __shared__ int wbase[LX * LY / 32], base;
   const int t = threadIdx.x, ntx = s.ntx, nty = s.nty, ntiles = ntx * nty;
-  const int tile = blockIdx.x * blockDim.x + t;
+  const int bx = blockIdx.x * LX, by = blockIdx.y * LY;
+  for (int q = t; q < (LY + 4) * (LX + 4); q += LX * LY) {
+    const int ly = q / (LX + 4), lx = q - ly * (LX + 4), gx = bx - 2 + lx, gy = by - 2 + ly;
+    rec[ly][lx] = (gx < 0 || gx >= ntx || gy < 0 || gy >= nty || s.odry_in[gy * ntx + gx] != 0) ? 1 : 0;
+  }
+  __syncthreads();
+  for (int q = t; q < (LY + 2) * (LX + 2); q += LX * LY) {
+    const int fy = q / (LX + 2), fx = q - fy * (LX + 2);
+    unsigned char d = 1;
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) d &= rec[fy + r][fx + c];
+    fs[fy][fx] = d;
+  }
+  __syncthreads();
+  const int lx = t % LX, ly = t / LX, tx = bx + lx, ty = by + ly;
   bool faces = false, cells = false;
-  if (tile < ntiles) {
-    const int tx = tile % ntx, ty = tile / ntx;
-    const bool settled = tile_face_settled(s.odry_in, ntx, nty, tx, ty);
+  if (tx < ntx && ty < nty) {
+    const int tile = ty * ntx + tx;
+    const bool settled = fs[ly + 1][lx + 1] != 0;
     if (settled) s.dry[tile] = 1;
     faces = !settled;
     cells = true;
@@ -525,17 +537,17 @@ __global__ void __launch_bounds__(256) k_face_list(SplitBufs s, Control* ctl, in
     const int i0 = tx * SPX, j0 = ty * SPY;
     if (cell_skip && settled && dt > 0 && dt < INFINITY && i0 >= 2 && i0 + SPX <= W - 2 && j0 >= 2 &&
         j0 + SPY <= H - 2 && s.odry_out[tile] == 2) {
-      bool all = true;
-      for (int r = -1; r <= 1 && all; r++)
-        for (int c = -1; c <= 1 && all; c++)
-          if (!(r == 0 && c == 0)) all = tile_face_settled(s.odry_in, ntx, nty, tx + c, ty + r);
+      unsigned char all = 1;
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) all &= fs[ly + r][lx + c];
       if (all) {
         cells = false;
         if ((tile & 15) == 0) atomicAdd(&ctl->settled_next, 1);
       }
     }
   }
-  if (blockIdx.x == 0 && t == 0) { *other_count = 0; *other_ccount = 0; }
+  if (blockIdx.x == 0 && blockIdx.y == 0 && t == 0) { *other_count = 0; *other_ccount = 0; }
+  const int tile = ty * ntx + tx;
   block_append(faces, tile, list, count, ntiles, wbase, &base);
   if (cell_skip) block_append(cells, tile, clist, ccount, ntiles, wbase, &base);   // uniform
 }
