@@ -592,22 +592,15 @@ def fma_build_summary(steps, warmup):
     return out
 
 
-def launches_per_step(swe, lib, sim, settling=True):
+def launches_per_step(swe, lib, sim):
     """Kernel launches of one step: prepare, two ghost fills and two stages
     of the stage kernels in use (the tiled pair per stage and one close of
     the step, or the fused kernel per stage)."""
     impl = ctypes.c_int(-1)
     swe._lib.check(lib.swe_get_stage_kernels(sim._h, ctypes.byref(impl)))
-    if impl.value != 1:
-        return 3 + 2
-    # with tensor-map tiles (an even padded width) and the settling cell kernel
-    # (a grid where tiles settle, as the beach) each face kernel is led by the
-    # kernel that lists the tiles the stage kernels must run
-    dims = (ctypes.c_int * 4)()
-    swe._lib.check(lib.swe_get_dims(sim._h, dims))
-    listed = (settling and dims[0] % 2 == 0 and os.environ.get("SWE_B200_TMA") != "0"
-              and os.environ.get("SWE_B200_FACE_LIST") != "0")
-    return 3 + 5 + (2 if listed else 0)
+    # the tiled pair per stage and one close; with tile lists each ghost fill
+    # makes the next stage's lists in the same launch
+    return 3 + (5 if impl.value == 1 else 2)
 
 
 def launch_cfg(swe, lib, sim):
@@ -838,7 +831,7 @@ def run_sphere(args):
     value = nx * ny * K / (ms / 1e3)
     dt_last = sim.maxDt()
     finite = sim.finite()
-    per_step = launches_per_step(swe, lib, sim, settling=False)   # too little land settles to keep it
+    per_step = launches_per_step(swe, lib, sim)
     sim.close()
     cpu = None
     if not args.no_cpu_baseline:

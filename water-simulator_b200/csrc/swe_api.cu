@@ -427,26 +427,46 @@ int ensure_split(swe_sim* s) {
 }
 
 
-// One stage (MODE 1 or 2) with the selected kernels.
+// The stage kernels' buffers of stage MODE (stage 1: A -> B, stage 2: B -> A).
 template <int MODE>
-int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
+swe::SplitBufs stage_bufs(const swe_sim* s) {
+  swe::SplitBufs sb = s->sb;
+  sb.odry_in = s->d_odry[MODE == 1 ? 0 : 1];
+  sb.odry_out = s->d_odry[MODE == 1 ? 1 : 0];
+  return sb;
+}
+// The tile lists pay where tiles settle: with the settling cell kernel
+// (which swe_run keeps only where a quarter or more of the tiles settle).
+bool stage_listed(const swe_sim* s) { return s->stage_impl == 1 && s->face_list && s->settle; }
+// Whether the cell kernel takes its list: when tiles may be left out.
+int cell_listed(const swe_sim* s, const swe::StageArgs& a) {
+  return stage_listed(s) && s->cell_tma && a.dryfold && a.minDepth >= 0 && a.sponge_width <= 0 && !a.h0c &&
+         !a.tape_th && !a.tape_hpre && !a.tape_pre[0];
+}
+template <int MODE>
+swe::TileLists tile_lists(const swe_sim* s, const swe::StageArgs& a) {
+  swe::TileLists L;
+  L.list = s->d_flist; L.count = s->d_fcount + (MODE - 1); L.other_count = s->d_fcount + (2 - MODE);
+  L.cell_skip = cell_listed(s, a);
+  L.clist = s->d_clist; L.ccount = s->d_ccount + (MODE - 1); L.other_ccount = s->d_ccount + (2 - MODE);
+  L.W = s->W; L.H = s->H;
+  return L;
+}
+
+// One stage (MODE 1 or 2) with the selected kernels; list_done: its lists
+// were made with the ghost fill (launch_bc_lists).
+template <int MODE>
+int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false, bool list_done = false) {
   if (s->stage_impl == 1) {
-    swe::SplitBufs sb = s->sb;                      // stage 1: A -> B, stage 2: B -> A
-    sb.odry_in = s->d_odry[MODE == 1 ? 0 : 1];
-    sb.odry_out = s->d_odry[MODE == 1 ? 1 : 0];
+    const swe::SplitBufs sb = stage_bufs<MODE>(s);
     const dim3 blk(swe::SP_THREADS);
-    // The tile lists pay where tiles settle: with the settling cell kernel
-    // (which swe_run keeps only where a quarter or more of the tiles settle).
-    const bool listed = s->face_list && s->settle;
-    const int cell_list = listed && s->cell_tma && sb.odry_out && a.dryfold && a.minDepth >= 0 &&
-                          a.sponge_width <= 0 && !a.h0c && !a.tape_th && !a.tape_hpre && !a.tape_pre[0];
+    const bool listed = stage_listed(s);
+    const int cell_list = cell_listed(s, a);
     if (listed) {
       const int ntiles = (int)(s->sgrid.x * s->sgrid.y);
-      const int cell_skip = cell_list;
-      CU(launch(pdl, swe::k_face_list, dim3((s->sgrid.x + swe::LX - 1) / swe::LX, (s->sgrid.y + swe::LY - 1) / swe::LY),
-                dim3(swe::LX * swe::LY), s->st, sb, s->d_ctl, s->d_flist,
-                s->d_fcount + (MODE - 1), s->d_fcount + (2 - MODE), cell_skip, s->d_clist,
-                s->d_ccount + (MODE - 1), s->d_ccount + (2 - MODE), s->W, s->H));
+      if (!list_done)
+        CU(launch(pdl, swe::k_face_list, dim3((s->sgrid.x + swe::LX - 1) / swe::LX, (s->sgrid.y + swe::LY - 1) / swe::LY),
+                  dim3(swe::LX * swe::LY), s->st, sb, s->d_ctl, tile_lists<MODE>(s, a)));
       CU(launch(pdl, swe::k_split_faces_tma_list, dim3(ntiles), blk, s->st, a, sb, s->d_ctl,
                 s->tmaps[MODE - 1], (const int*)s->d_flist, (const int*)(s->d_fcount + (MODE - 1))));
     } else if (s->tma) {
@@ -480,6 +500,20 @@ int launch_stage(swe_sim* s, const swe::StageArgs& a, bool pdl = false) {
   return SWE_OK;
 }
 
+// The ghost fill of f, and with tile lists the lists of stage MODE in the
+// same launch (k_bc_face_list); returns through `listed` whether it made them.
+template <int MODE>
+int launch_bc_lists(swe_sim* s, double* const* f, int respect_stop, bool pdl, const swe::StageArgs& a,
+                    bool& listed) {
+  listed = stage_listed(s);
+  if (!listed) return launch_bc(s, f, respect_stop, pdl);
+  const int nbc = bc_blocks(s);
+  const int nrx = (s->sgrid.x + swe::LX - 1) / swe::LX, nry = (s->sgrid.y + swe::LY - 1) / swe::LY;
+  CU(launch(pdl, swe::k_bc_face_list, dim3(nbc + nrx * nry), dim3(swe::LX * swe::LY), s->st, bc_args(s, f),
+            respect_stop, nbc, stage_bufs<MODE>(s), s->d_ctl, tile_lists<MODE>(s, a), nrx));
+  return SWE_OK;
+}
+
 int enqueue_step(swe_sim* s, int mode, double dt, double t_end, const double* dt_dev = nullptr) {
   // The tiled kernels, the ghost fills and prepare enter through pdl_enter,
   // so each may be scheduled while its predecessor drains.
@@ -488,16 +522,17 @@ int enqueue_step(swe_sim* s, int mode, double dt, double t_end, const double* dt
   // Host-checked dt (mode 0) never reaches here refused.  In the device loop
   // a refused step (t reached t_end) changes nothing, ghosts included, as the
   // drivers' `while (sim.t < T)` loop stops calling step().
-  int rc = launch_bc(s, s->d_A, mode == 0 ? 0 : 1, pdl);
-  if (rc) return rc;
   swe::StageArgs a1 = stage_args(s, s->d_A, s->d_B);
-  rc = launch_stage<1>(s, a1, pdl);
+  bool listed = false;
+  int rc = launch_bc_lists<1>(s, s->d_A, mode == 0 ? 0 : 1, pdl, a1, listed);
   if (rc) return rc;
-  rc = launch_bc(s, s->d_B, 1, pdl);
+  rc = launch_stage<1>(s, a1, pdl, listed);
   if (rc) return rc;
   swe::StageArgs a2 = stage_args(s, s->d_B, s->d_A);
   if (s->keep_h0) { a2.h0c = s->d_h0[0]; a2.hu0c = s->d_h0[1]; a2.hv0c = s->d_h0[2]; }
-  return launch_stage<2>(s, a2, pdl);
+  rc = launch_bc_lists<2>(s, s->d_B, 1, pdl, a2, listed);
+  if (rc) return rc;
+  return launch_stage<2>(s, a2, pdl, listed);
 }
 
 // Blocks of a grid-stride reduction over `cells` cells: one per 256 cells,

@@ -503,15 +503,22 @@ __device__ __forceinline__ void block_append(bool on, int value, int* list, int*
 // test of the region and one tile around it is made there, and each thread
 // then decides for its own tile.
 constexpr int LX = 32, LY = 8;                     // tiles per list CTA
-__global__ void __launch_bounds__(LX * LY) k_face_list(SplitBufs s, Control* ctl, int* list, int* count,
-                                                       int* other_count, int cell_skip, int* clist, int* ccount,
-                                                       int* other_ccount, int W, int H) {
-  pdl_enter();
+struct TileLists {
+  int* list; int* count; int* other_count;         // the face kernel's
+  int cell_skip;
+  int* clist; int* ccount; int* other_ccount;      // the cell kernel's
+  int W, H;
+};
+// The lists of the region (rx, ry) of tiles; every thread of the CTA calls it.
+__device__ __forceinline__ void face_list_region(const SplitBufs& s, Control* ctl, const TileLists& L, int rx,
+                                                 int ry) {
   __shared__ unsigned char rec[LY + 4][LX + 4];      // record dry (or outside the grid)
   __shared__ unsigned char fs[LY + 2][LX + 2];       // settles in the face kernel
   __shared__ int wbase[LX * LY / 32], base;
+  int* const list = L.list; int* const count = L.count; int* const clist = L.clist; int* const ccount = L.ccount;
+  const int cell_skip = L.cell_skip, W = L.W, H = L.H;
   const int t = threadIdx.x, ntx = s.ntx, nty = s.nty, ntiles = ntx * nty;
-  const int bx = blockIdx.x * LX, by = blockIdx.y * LY;
+  const int bx = rx * LX, by = ry * LY;
   for (int q = t; q < (LY + 4) * (LX + 4); q += LX * LY) {
     const int ly = q / (LX + 4), lx = q - ly * (LX + 4), gx = bx - 2 + lx, gy = by - 2 + ly;
     rec[ly][lx] = (gx < 0 || gx >= ntx || gy < 0 || gy >= nty || s.odry_in[gy * ntx + gx] != 0) ? 1 : 0;
@@ -546,10 +553,29 @@ __global__ void __launch_bounds__(LX * LY) k_face_list(SplitBufs s, Control* ctl
       }
     }
   }
-  if (blockIdx.x == 0 && blockIdx.y == 0 && t == 0) { *other_count = 0; *other_ccount = 0; }
+  if (rx == 0 && ry == 0 && t == 0) { *L.other_count = 0; *L.other_ccount = 0; }
   const int tile = ty * ntx + tx;
   block_append(faces, tile, list, count, ntiles, wbase, &base);
   if (cell_skip) block_append(cells, tile, clist, ccount, ntiles, wbase, &base);   // uniform
+}
+__global__ void __launch_bounds__(LX * LY) k_face_list(SplitBufs s, Control* ctl, TileLists L) {
+  pdl_enter();
+  face_list_region(s, ctl, L, blockIdx.x, blockIdx.y);
+}
+// The ghost fill of the stage's input (its first nbc blocks, as k_apply_bc)
+// and the stage's lists (the other blocks, one per region of nrx columns of
+// regions) in one launch: the lists read only the records, the fill only
+// the state.
+__global__ void __launch_bounds__(LX * LY) k_bc_face_list(BCArgs b, int respect_stop, int nbc, SplitBufs s,
+                                                          Control* ctl, TileLists L, int nrx) {
+  pdl_enter();
+  if ((int)blockIdx.x < nbc) {                     // uniform per block
+    if (respect_stop && ctl->stop) return;
+    apply_bc_range(b, ctl, blockIdx.x * blockDim.x + threadIdx.x, nbc * blockDim.x);
+    return;
+  }
+  const int r = blockIdx.x - nbc;
+  face_list_region(s, ctl, L, r % nrx, r / nrx);
 }
 
 // The face kernel over the list: CTA b computes the list's entry b, and the
