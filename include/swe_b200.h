@@ -221,6 +221,9 @@ int swe_set_diag_order(swe_sim* s, int order);
 int swe_eta_projection(swe_sim* s, const double* coef, double* out);
 int swe_max_speed(swe_sim* s, double* out);
 int swe_finite(swe_sim* s, int* out);
+/* Waits for the handle's stream.  SWE_ETIMEOUT when a tile copy of the
+ * stepping kernels did not complete within its time bound since the last
+ * call (that tile was left unwritten, so those steps are incomplete). */
 int swe_synchronize(swe_sim* s);
 /* The handle's CUDA stream (a cudaStream_t), so a caller can record CUDA
  * events on the stream the kernels run on. */

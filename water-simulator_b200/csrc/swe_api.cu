@@ -1352,6 +1352,19 @@ int swe_get_stage_kernels(swe_sim* s, int* impl) {
 int swe_synchronize(swe_sim* s) {
   if (!s) return fail(SWE_EINVAL, "null argument");
   CU(cudaStreamSynchronize(s->st));
+  // A tile copy that did not complete within its bound left its tile
+  // unwritten and set bit 4 of the control block's status
+  // (swe_split.cuh): reported here once, then cleared.
+  int st = 0;
+  CU(cudaMemcpyAsync(&st, &s->d_ctl->status, sizeof st, cudaMemcpyDeviceToHost, s->st));
+  CU(cudaStreamSynchronize(s->st));
+  if (st & 4) {
+    const int cleared = st & ~4;
+    CU(cudaMemcpyAsync(&s->d_ctl->status, &cleared, sizeof cleared, cudaMemcpyHostToDevice, s->st));
+    CU(cudaStreamSynchronize(s->st));
+    return fail(SWE_ETIMEOUT, "swe_synchronize: a tile copy did not complete within its time bound; the steps "
+                              "since the last synchronize are incomplete");
+  }
   return SWE_OK;
 }
 

@@ -57,7 +57,7 @@ struct Control {
   // tiles the tiled cell kernels settled in the last step, one in 16
   // counted; beside `stop` and `dt`, in the line every kernel reads first
   int settled;
-  int status;           // sticky status bits (1: non-finite CFL rate seen)
+  int status;           // sticky status bits (4: a tile copy did not complete within its bound)
   unsigned int counter; // last-CTA ticket
   // Flather tide tables (src/tide.mjs:103-107), per side
   int tide_n[4];
